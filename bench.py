@@ -1,0 +1,346 @@
+"""Benchmark of the tinyMD B200 timestep: LJ atom-steps/s on one B200.
+
+Workload (the configuration the metric is quoted on): LJ 'default' FCC
+lattice of 32x32x32 unit cells (131,072 atoms, lattice constant 1.6796),
+velocities from the per-site Park-Miller seeds rescaled to T = 1.44,
+eps = sigma = 1, cutoff 2.5, skin 0.3, dt 0.005, reneighbour every 20 steps,
+full neighbour lists.  A "step" is one MD timestep (main.cpp:715-776).
+
+value   atom-steps/s of the mixed form (FP64 state / FP32 pair forces) over K
+        device-timed steps (CUDA events around each step on the library's
+        stream; the 131k working set fits in L2, so L2 is flushed by writing a
+        256 MiB buffer before every timed step, outside the timed interval).
+forms   the FP64 form's atom-steps/s on the same workload, the ratio, and the
+        mixed form's max force error / rms force against FP64 positions.
+e2e     the same metric through the C ABI with host buffers: md_initialize_grid
+        from host arrays, upload, K steps, download and md_write_grid_data_to_arrays,
+        timed on the host clock around the whole run.
+roofline  the mixed force kernel: algorithmic bytes per launch / average
+        launch time (CUDA events around each force launch) against the
+        measured HBM bandwidth.
+cpu_baseline  the CPU oracle (a restatement of the reference's cpu backend)
+        timed on this host over a bounded sample of the same workload.
+
+--impl reference runs that CPU path alone (all host threads) on the same
+workload and prints the same JSON line.  Under torchrun each rank runs an
+independent replica (the path does not shard); value sums the replicas and
+uses the max time over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "molecular-dynamics_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "LJ atom-steps/s, 1 B200: mixed-FP32 vs FP64 at stated error; adjoint/fwd time"
+UNIT = "atom-steps/s"
+CELLS = (32, 32, 32)
+DT = 0.005
+L2_FLUSH_BYTES = 256 << 20
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def measured_traffic():
+    """Per-launch DRAM bytes of the mixed force kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "force_lj_mixed_131k.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get("dram_bytes_per_launch")
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.file:
+            return None
+        self.file.flush()
+        rows = []
+        with open(self.file.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_info():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def dist_init(world, backend):
+    import torch.distributed as dist
+    if world > 1 and not dist.is_initialized():
+        import datetime
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist if world > 1 else None
+
+
+def allreduce_max(x, dist, device=None):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+def cpu_run(steps, threads, cells=CELLS, warmup=1):
+    """The oracle's CPU path on `threads` host threads; returns (atom-steps/s, atoms, seconds)."""
+    import tinymd
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+    ora = tinymd.open_library(os.path.join(ROOT, "oracle", "_build", "libtinymd_oracle.so"))
+    ora.oracle_set_threads(threads)
+    setup_lib = tinymd.load(build_if_missing=True)
+    m, x, v, world, rank = tinymd.setup_particles("default", cells, lib=setup_lib)
+    sim = tinymd.Simulation(ora, m, x, v, world, rank, temp=1.44)
+    sim.step(DT, warmup)
+    t0 = time.perf_counter()
+    sim.step(DT, steps)
+    t = time.perf_counter() - t0
+    sim.close()
+    return len(m) * steps / t, len(m), t
+
+
+def run_reference(args):
+    rank, world, local = dist_info()
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    steps = args.steps
+    rate, natoms, secs = cpu_run(steps, threads, warmup=min(args.warmup, 20))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded FCC lattice, reference Park-Miller velocities)",
+        "config": {"workload": "lj_default_fcc_32x32x32_131072_atoms_full_list", "atoms": natoms, "dt": DT,
+                   "reneigh": 20, "cutoff": 2.5, "skin": 0.3},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{natoms} atoms x {steps} timesteps (full workload), OpenMP over atoms"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_steps(tm, lib, sim, steps, flush):
+    """Device time of `steps` steps, each bracketed by CUDA events, L2 flushed before each."""
+    import torch
+    st = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    launches0 = lib.md_kernel_launches()
+    for k in range(steps):
+        flush.zero_()
+        ev[k][0].record(st)
+        sim.step(DT, 1)
+        ev[k][1].record(st)
+    lib.md_synchronize()
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    return ms, lib.md_kernel_launches() - launches0
+
+
+def run_ours(args):
+    import torch
+    import tinymd as tm
+    rank, world, local = dist_info()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = dist_init(world, "nccl")
+    lib = tm.load()
+    lib.md_set_stream(ctypes_stream(torch.cuda.current_stream()))
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    parts = tm.setup_particles("default", CELLS, lib=lib)
+    natoms = len(parts[0])
+    K, W = args.steps, args.warmup
+    result = {}
+
+    # ---- FP64 form ---------------------------------------------------------------
+    lib.md_set_precision(0)
+    sim = tm.Simulation(lib, *parts, temp=1.44)
+    sim.step(DT, W)
+    barrier(dist)
+    ms64, _ = timed_steps(tm, lib, sim, K, flush)
+    sim.close()
+    ms64 = allreduce_max(ms64, dist, dev)
+
+    # ---- mixed form (headline) ----------------------------------------------------
+    lib.md_set_precision(1)
+    sim = tm.Simulation(lib, *parts, temp=1.44)
+    sim.step(DT, W)
+    lib.md_profile_enable(1 << 0)  # events around the LJ force launches
+    lib.md_profile_reset()
+    barrier(dist)
+    with ClockSampler(local) as clk:
+        ms32, launches = timed_steps(tm, lib, sim, K, flush)
+    clocks = clk.summary()
+    nl = ctypes.c_longlong()
+    fms = ctypes.c_double()
+    lib.md_profile_get(0, ctypes.byref(nl), ctypes.byref(fms))
+    lib.md_profile_enable(0)
+    # mean list length of the current lists (full list, FP64 cutoff 2.8)
+    sizes = np.zeros(natoms, dtype=np.int32)
+    lists = np.zeros((natoms, 1), dtype=np.int32)
+    lib.md_get_neighbor_lists(tm.ptr(sizes), tm.ptr(lists), 1)
+    mean_nb = float(sizes.mean())
+    # force error of the mixed form on the FP64 form's positions (same state)
+    _, _, f32 = tm.full_state(lib)
+    lib.md_set_precision(0)
+    sim.force()
+    lib.md_final_integration(0.0)
+    _, _, f64 = tm.full_state(lib)
+    ferr = float(np.max(np.abs(f32 - f64)) / np.sqrt(np.mean(f64 ** 2)))
+    sim.close()
+    ms32 = allreduce_max(ms32, dist, dev)
+
+    # ---- end to end through the C ABI with host buffers ---------------------------
+    lib.md_set_precision(1)
+    m, x, v, world_box, rank_box = parts
+    e2e_runs = []
+    for rep in range(2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s = tm.Simulation(lib, m, x, v, world_box, rank_box, temp=1.44)
+        s.step(DT, K)
+        mm, xx, vv, ff = s.arrays()
+        t1 = time.perf_counter()
+        s.close()
+        e2e_runs.append(t1 - t0)
+    e2e_s = allreduce_max(min(e2e_runs), dist, dev)
+    lib.md_set_precision(0)
+    h2d = natoms * (8 + 24 + 24)
+    d2h = (natoms + sim_ghosts_estimate(natoms)) * (32 * 3 + 8 + 16 + 4)
+
+    total_atoms = natoms * world
+    value = total_atoms * K / (ms32 * 1e-3)
+    value64 = total_atoms * K / (ms64 * 1e-3)
+    peak, peak_kind = peaks()
+    force_ms = fms.value / max(nl.value, 1)
+    bytes_per_atom = 4 + mean_nb * (4 + 16) + 16 + 16  # count, list entry + float4 gather, own float4 pos, float4 force
+    achieved = natoms * bytes_per_atom / (force_ms * 1e-3) / 1e9
+    traffic = measured_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms32 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 state + f32 pair forces (mixed form)",
+        "data": "synthetic (seeded FCC lattice, reference Park-Miller velocities)",
+        "config": {"workload": "lj_default_fcc_32x32x32_131072_atoms_full_list", "atoms_per_gpu": natoms,
+                   "dt": DT, "reneigh": 20, "cutoff": 2.5, "skin": 0.3, "l2": "flushed before every timed step",
+                   "parallelism": f"replicas x{world}"},
+        "forms": {"mixed": value, "fp64": value64, "mixed_over_fp64": value / value64,
+                  "mixed_max_force_err_over_rms": ferr},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
+                     "bytes_per_atom": bytes_per_atom, "mean_list_length": mean_nb,
+                     "launch_ms": force_ms, "launches": nl.value},
+        "e2e": {"value": total_atoms * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+                "d2h_bytes_per_step": d2h / K,
+                "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        steps = 40
+        rate, n_cpu, secs = cpu_run(steps, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{n_cpu} atoms x {steps} timesteps of the same workload"}
+    if dist is not None:
+        barrier(dist)
+        import torch.distributed as td
+        td.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def sim_ghosts_estimate(n):
+    return int(0.4 * n)
+
+
+def ctypes_stream(s):
+    return ctypes.c_void_p(s.cuda_stream)
+
+
+import ctypes  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,1088 @@
+// api.cu -- the md_* C ABI of the tinyMD B200 library (host orchestration).
+//
+// Replaces the runtime of core/runtime.impala for one process on one GPU.
+// The reference synchronises after every kernel (backend/mapping_gpu.impala:
+// 12-27); here calls enqueue on one stream and adjacent calls of a timestep
+// are fused:
+//   md_initial_integration + md_synchronize_ghost_layer -> one kernel
+//   md_compute_lennard_jones (full list) + md_final_integration -> one kernel
+// Every call that exposes data to the host drains pending work first.
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <vector>
+
+#include "md_common.cuh"
+#include "md_state.h"
+#include "tinymd_b200.h"
+
+namespace tmd {
+
+State g_state;
+
+// ---------------------------------------------------------------------------
+// errors, launches, memory
+// ---------------------------------------------------------------------------
+void set_error(int code, const std::string& msg) {
+    g_state.last_error = code;
+    g_state.last_error_msg = msg;
+    std::fprintf(stderr, "tinymd_b200: %s\n", msg.c_str());
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return true;
+    set_error(MD_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return false;
+}
+
+void launched(int kernel_id) {
+    (void)kernel_id;
+    g_state.launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) set_error(MD_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
+void dev_alloc(void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (cuda_ok(cudaMalloc(p, bytes), "cudaMalloc")) g_state.dev_bytes += (long long)bytes;
+}
+
+void dev_free(void** p) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+}
+
+const char* kernel_name(int id) {
+    static const char* names[K_COUNT] = {"force_lj", "force_dem", "integrate", "ghost_sync", "final_integrate",
+                                         "enforce_pbc", "borders", "binning", "neighbor_list", "scan", "reduce",
+                                         "adjoint_hvp", "adjoint_step", "misc"};
+    return (id >= 0 && id < K_COUNT) ? names[id] : "?";
+}
+
+// ---------------------------------------------------------------------------
+// GPU phase timeline (CUDA events at phase changes on the library stream)
+// ---------------------------------------------------------------------------
+namespace {
+struct Mark {
+    cudaEvent_t ev;
+    int phase;
+};
+std::vector<cudaEvent_t> ev_pool;
+std::deque<Mark> marks;
+double phase_ms[PH_COUNT] = {0};
+int cur_phase = 0;
+
+struct ProfRec {
+    cudaEvent_t a, b;
+    int k;
+};
+std::deque<ProfRec> prof_q;
+long long prof_launch[K_COUNT] = {0};
+double prof_ms[K_COUNT] = {0};
+int prof_mask = 0;
+cudaEvent_t prof_open[K_COUNT] = {nullptr};
+
+cudaEvent_t get_event() {
+    if (!ev_pool.empty()) {
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    TMD_CUDA(cudaEventCreate(&e));
+    return e;
+}
+void put_event(cudaEvent_t e) { ev_pool.push_back(e); }
+
+void fold_marks(bool all) {
+    while (marks.size() >= 2) {
+        const Mark& a = marks[0];
+        const Mark& b = marks[1];
+        if (!all && cudaEventQuery(b.ev) != cudaSuccess) break;
+        if (all) cudaEventSynchronize(b.ev);
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, a.ev, b.ev) == cudaSuccess && a.phase > 0 && a.phase < PH_COUNT)
+            phase_ms[a.phase] += ms;
+        put_event(a.ev);
+        marks.pop_front();
+    }
+}
+
+void fold_prof(bool all) {
+    while (!prof_q.empty()) {
+        ProfRec& r = prof_q.front();
+        if (!all && cudaEventQuery(r.b) != cudaSuccess) break;
+        if (all) cudaEventSynchronize(r.b);
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess) {
+            prof_ms[r.k] += ms;
+            prof_launch[r.k]++;
+        }
+        put_event(r.a);
+        put_event(r.b);
+        prof_q.pop_front();
+    }
+}
+}  // namespace
+
+void phase_mark(int phase) {
+    if (phase == cur_phase) return;
+    cudaEvent_t e = get_event();
+    TMD_CUDA(cudaEventRecord(e, g_state.stream));
+    marks.push_back({e, phase});
+    cur_phase = phase;
+    if (marks.size() > 512) fold_marks(false);
+}
+
+void phase_times(double* out6) {
+    cudaEvent_t e = get_event();
+    TMD_CUDA(cudaEventRecord(e, g_state.stream));
+    marks.push_back({e, cur_phase});
+    fold_marks(true);
+    double tot = 0;
+    for (int p = 1; p < PH_COUNT; ++p) tot += phase_ms[p];
+    out6[0] = tot;
+    out6[1] = phase_ms[PH_FORCE];
+    out6[2] = phase_ms[PH_NEIGH];
+    out6[3] = phase_ms[PH_COMM];
+    out6[4] = phase_ms[PH_BALANCE];
+    out6[5] = phase_ms[PH_OTHER];
+}
+
+void phase_reset() {
+    fold_marks(true);
+    for (auto& m : marks) put_event(m.ev);
+    marks.clear();
+    for (double& v : phase_ms) v = 0;
+    cur_phase = 0;
+}
+
+void prof_begin(int k) {
+    if (!(prof_mask & (1 << k))) return;
+    prof_open[k] = get_event();
+    TMD_CUDA(cudaEventRecord(prof_open[k], g_state.stream));
+}
+
+void prof_end(int k) {
+    if (!(prof_mask & (1 << k)) || !prof_open[k]) return;
+    cudaEvent_t b = get_event();
+    TMD_CUDA(cudaEventRecord(b, g_state.stream));
+    prof_q.push_back({prof_open[k], b, k});
+    prof_open[k] = nullptr;
+    if (prof_q.size() > 512) fold_prof(false);
+}
+
+void prof_reset() {
+    fold_prof(true);
+    for (int k = 0; k < K_COUNT; ++k) {
+        prof_launch[k] = 0;
+        prof_ms[k] = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class T>
+void realloc_keep(T** p, size_t old_n, size_t new_n, cudaStream_t st) {
+    T* q = nullptr;
+    dalloc(&q, new_n);
+    if (*p && old_n) TMD_CUDA(cudaMemcpyAsync(q, *p, sizeof(T) * std::min(old_n, new_n), cudaMemcpyDeviceToDevice, st));
+    if (*p) {
+        TMD_CUDA(cudaStreamSynchronize(st));
+        dfree(p);
+    }
+    *p = q;
+}
+
+int border_blocks(int N) { return (N + 255) / 256; }
+
+void free_all(State& s) {
+    for (int b = 0; b < 2; ++b) {
+        dfree(&s.pos.b[b]);
+        dfree(&s.vel.b[b]);
+        dfree(&s.frc.b[b]);
+        dfree(&s.mass.b[b]);
+        dfree(&s.ref.b[b]);
+        dfree(&s.img.b[b]);
+    }
+    int** ip[] = {&s.rbk, &s.slot_of_ref, &s.gsrc, &s.groot, &s.gcode, &s.cnt, &s.cstart, &s.bin_cell,
+                  &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.bcount, &s.bsrc_ref, &s.broot_ref, &s.bcode,
+                  &s.nbn, &s.scan_part};
+    for (int** q : ip) dfree(q);
+    dfree(&s.frc32);
+    dfree(&s.pos32);
+    dfree(&s.bmask);
+    dfree(&s.nbl);
+    dfree(&s.red_part);
+    dfree(&s.thermo_dev);
+    dfree(&s.status_dev);
+    s.scan_part_cap = 0;
+    s.red_part_cap = 0;
+    s.dev_bytes = 0;
+}
+
+}  // namespace
+
+// grows every per-slot array to hold `need` slots, keeping contents
+void grow_atoms(State& s, int need) {
+    const int oldc = s.capA;
+    const int newc = need + need / 10 + 1024;
+    const size_t o = (size_t)oldc, n = (size_t)newc;
+    for (int b = 0; b < 2; ++b) {
+        realloc_keep(&s.pos.b[b], o, n, s.stream);
+        realloc_keep(&s.vel.b[b], o, n, s.stream);
+        realloc_keep(&s.frc.b[b], o, n, s.stream);
+        realloc_keep(&s.mass.b[b], o, n, s.stream);
+        realloc_keep(&s.ref.b[b], o, n, s.stream);
+        realloc_keep(&s.img.b[b], o, n, s.stream);
+    }
+    realloc_keep(&s.frc32, o, n, s.stream);
+    realloc_keep(&s.pos32, o, n, s.stream);
+    int** keep[] = {&s.rbk, &s.slot_of_ref, &s.gsrc, &s.groot, &s.gcode, &s.bsrc_ref, &s.broot_ref, &s.bcode};
+    for (int** q : keep) realloc_keep(q, o, n, s.stream);
+    int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.nbn};
+    for (int** q : scratch) {
+        dfree(q);
+        dalloc(q, n);
+    }
+    s.capA = newc;
+    if (oldc > 0) std::printf("0> reallocate_particle_capacity(): %d\n", newc);
+}
+
+void grow_lists(State& s, int rows) {
+    dfree(&s.nbl);
+    s.nb_cap = rows;
+    dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+    s.lists_valid = 0;
+}
+
+namespace {
+
+void allocate_state(State& s, int N, int nb_cap) {
+    s.capA = 0;
+    grow_atoms(s, N + N / 2 + 64);
+    const int ncells = s.geo.ncells;
+    const int nseg = 2 * (ncells + 1);
+    dalloc(&s.cnt, nseg + 1);
+    dalloc(&s.cstart, nseg + 1);
+    dalloc(&s.bmask, (size_t)std::max(N, 1));
+    const int nblk = border_blocks(std::max(N, 1));
+    dalloc(&s.bcount, (size_t)2 * 26 * nblk + 1);
+    s.nb_stride = ((std::max(N, 1) + 31) / 32) * 32;
+    s.nb_cap = nb_cap > 0 ? nb_cap : 100;
+    dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+    dalloc(&s.thermo_dev, 8);
+    dalloc(&s.status_dev, 1);
+    if (!s.status_host) TMD_CUDA(cudaMallocHost((void**)&s.status_host, sizeof(DevStatus)));
+    if (!s.thermo_host) TMD_CUDA(cudaMallocHost((void**)&s.thermo_host, 8 * sizeof(double)));
+    TMD_CUDA(cudaMemsetAsync(s.status_dev, 0, sizeof(DevStatus), s.stream));
+    TMD_CUDA(cudaMemsetAsync(s.thermo_dev, 0, 8 * sizeof(double), s.stream));
+    ensure_scan_scratch(s, std::max(nseg, 26 * nblk));
+}
+
+bool require_alive(const char* what) {
+    if (!g_state.alive) {
+        set_error(MD_ERR_STATE, std::string(what) + " called before md_initialize_grid");
+        return false;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// deferred work
+// ---------------------------------------------------------------------------
+void launch_force(State& s, const PendingForce& p, bool fuse_final, double dt) {
+    s.last_force_half = p.half ? 1 : 0;
+    if (p.dem) run_force_dem(s, p);
+    else run_force_lj(s, p, fuse_final, dt);
+}
+
+void flush_init(State& s) {
+    if (!s.pend_init) return;
+    s.pend_init = false;
+    phase_mark(PH_FORCE);
+    run_integrate(s, s.pend_dt, false);
+}
+
+void flush_force(State& s) {
+    if (!s.pend_force.valid) return;
+    PendingForce p = s.pend_force;
+    s.pend_force.valid = false;
+    phase_mark(PH_FORCE);
+    launch_force(s, p, false, 0.0);
+}
+
+void flush_all(State& s) {
+    flush_init(s);
+    flush_force(s);
+}
+
+void sync_stream(State& s) { TMD_CUDA(cudaStreamSynchronize(s.stream)); }
+
+// pinned staging area for host <-> device copies
+void* stage_ptr = nullptr;
+size_t stage_bytes = 0;
+void* stage(size_t bytes) {
+    if (bytes > stage_bytes) {
+        if (stage_ptr) cudaFreeHost(stage_ptr);
+        stage_ptr = nullptr;
+        stage_bytes = bytes + (bytes >> 3) + 4096;
+        if (!TMD_CUDA(cudaMallocHost(&stage_ptr, stage_bytes))) stage_bytes = 0;
+    }
+    return stage_ptr;
+}
+
+__global__ void k_iota(int* a, int* b, int* img, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        a[i] = i;
+        b[i] = i;
+        img[i] = 0;
+    }
+}
+
+__global__ void k_convert_forces(double4* f64, float4* f32, int n, int to32) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (to32) {
+        double4 f = f64[i];
+        f32[i] = make_float4((float)f.x, (float)f.y, (float)f.z, 0.f);
+    } else {
+        float4 f = f32[i];
+        f64[i] = make_double4(f.x, f.y, f.z, 0.0);
+    }
+}
+
+// downloads slot data and scatters it to reference order
+struct Snapshot {
+    std::vector<double4> pos, vel, frc;
+    std::vector<float4> frc32;
+    std::vector<double> mass;
+    std::vector<int> ref;
+};
+
+void snapshot(State& s, Snapshot& sn) {
+    flush_all(s);
+    const int NA = s.N + s.G;
+    sn.pos.resize(NA);
+    sn.vel.resize(NA);
+    sn.frc.resize(NA);
+    sn.frc32.resize(NA);
+    sn.mass.resize(NA);
+    sn.ref.resize(NA);
+    if (NA == 0) return;
+    TMD_CUDA(cudaMemcpyAsync(sn.pos.data(), s.pos.b[s.pc], sizeof(double4) * NA, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(sn.vel.data(), s.vel.b[s.vc], sizeof(double4) * NA, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(sn.frc.data(), s.frc.b[s.ac], sizeof(double4) * NA, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(sn.frc32.data(), s.frc32, sizeof(float4) * NA, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(sn.mass.data(), s.mass.b[s.ac], sizeof(double) * NA, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(sn.ref.data(), s.ref.b[s.ac], sizeof(int) * NA, cudaMemcpyDeviceToHost, s.stream));
+    sync_stream(s);
+}
+
+// std::cout default formatting of a double (6 significant digits)
+void print_g(double v) { std::printf("%g", v); }
+
+double host_temperature(const State& s) {  // core/thermo.impala:1-16 on the host mirror
+    const double mass = 1.0, mvv2e = 1.0;
+    int dof = s.N * 3 - 3;
+    double t_scale = mvv2e / (double)dof;
+    double t = 0.0;
+    for (int i = 0; i < s.N; ++i) {
+        const double* v = &s.h_vel[(size_t)i * 3];
+        t += (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * mass;
+    }
+    return t * t_scale;
+}
+
+}  // namespace
+}  // namespace tmd
+
+using namespace tmd;
+
+extern "C" {
+
+int md_last_error(void) { return g_state.last_error; }
+const char* md_last_error_string(void) { return g_state.last_error_msg.c_str(); }
+void md_clear_error(void) {
+    g_state.last_error = 0;
+    g_state.last_error_msg.clear();
+}
+
+void md_set_stream(void* stream) {
+    State& s = g_state;
+    if (s.alive) flush_all(s);
+    if (s.own_stream && s.stream) {
+        cudaStreamSynchronize(s.stream);
+        cudaStreamDestroy(s.stream);
+    }
+    s.stream = (cudaStream_t)stream;
+    s.own_stream = false;
+}
+
+// core/runtime.impala:7-37
+int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D const* velocities, int n,
+                       double const* aabb, double const* rank_aabb, double cell_spacing, int cell_capacity,
+                       int neighborlist_capacity) {
+    (void)cell_capacity;  // cells are a counting sort here: no per-cell capacity
+    State& s = g_state;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        set_error(MD_ERR_NO_DEVICE, "no CUDA device available");
+        return -1;
+    }
+    if (n < 0 || n >= kMaxSlots / 2 || !(cell_spacing > 0.0)) {
+        set_error(MD_ERR_ARGUMENT, "md_initialize_grid: invalid particle count or cell spacing");
+        return -1;
+    }
+    if (s.alive) md_deallocate_grid();
+    TMD_CUDA(cudaGetDevice(&s.device));
+    if (!s.stream) {
+        TMD_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        s.own_stream = true;
+    }
+    Geometry& g = s.geo;
+    for (int d = 0; d < 3; ++d) {
+        g.world_lo[d] = aabb[2 * d];
+        g.world_hi[d] = aabb[2 * d + 1];
+        g.aabb_lo[d] = rank_aabb[2 * d] - cell_spacing;
+        g.aabb_hi[d] = rank_aabb[2 * d + 1] + cell_spacing;
+        g.len[d] = g.world_hi[d] - g.world_lo[d];
+    }
+    g.spacing = cell_spacing;
+    // core/grid.impala:94-98
+    g.nx = (int)std::floor((g.aabb_hi[0] - g.aabb_lo[0] + (cell_spacing / 2.0)) / cell_spacing) + 1;
+    g.ny = (int)std::floor((g.aabb_hi[1] - g.aabb_lo[1] + (cell_spacing / 2.0)) / cell_spacing) + 1;
+    g.nz = (int)std::floor((g.aabb_hi[2] - g.aabb_lo[2] + (cell_spacing / 2.0)) / cell_spacing) + 1;
+    g.ncells = g.nx * g.ny * g.nz;
+    // dyadic rebasing grid strictly wider than the cell spacing (mixed form)
+    g.rb_h = (std::floor(cell_spacing * 8.0) + 1.0) / 8.0;
+
+    s.N = n;
+    s.G = 0;
+    s.pc = s.vc = s.ac = 0;
+    s.lists_valid = 0;
+    s.pend_init = false;
+    s.pend_force = PendingForce();
+    s.force_iters = s.rsq_iters = s.integration_iters = 0;
+    s.launches = 0;
+    allocate_state(s, n, neighborlist_capacity);
+
+    // core/grid.impala:215-249: the host mirror in input order
+    s.h_mass.assign(masses, masses + n);
+    s.h_pos.resize((size_t)n * 3);
+    s.h_vel.resize((size_t)n * 3);
+    s.h_frc.assign((size_t)n * 3, 0.0);
+    for (int i = 0; i < n; ++i) {
+        s.h_pos[3 * i + 0] = positions[i].x;
+        s.h_pos[3 * i + 1] = positions[i].y;
+        s.h_pos[3 * i + 2] = positions[i].z;
+        s.h_vel[3 * i + 0] = velocities[i].x;
+        s.h_vel[3 * i + 1] = velocities[i].y;
+        s.h_vel[3 * i + 2] = velocities[i].z;
+    }
+    s.h_x0 = s.h_pos;
+    s.alive = true;
+    phase_reset();
+    return s.N;
+}
+
+// core/runtime.impala:158-186 (host mirror, sequential sums as the reference)
+void md_create_velocity(double t_request) {
+    State& s = g_state;
+    if (!require_alive("md_create_velocity")) return;
+    const int n = s.N;
+    double vt[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) vt[d] = vt[d] + s.h_vel[3 * i + d];
+    for (int d = 0; d < 3; ++d) vt[d] = vt[d] / (double)n;
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) s.h_vel[3 * i + d] = s.h_vel[3 * i + d] - vt[d];
+    double t = host_temperature(s);
+    double factor = std::sqrt(t_request / t);
+    for (int i = 0; i < n; ++i)
+        for (int d = 0; d < 3; ++d) s.h_vel[3 * i + d] = s.h_vel[3 * i + d] * factor;
+}
+
+// core/grid.impala:360-367
+void md_copy_data_to_accelerator(void) {
+    State& s = g_state;
+    if (!require_alive("md_copy_data_to_accelerator")) return;
+    flush_all(s);
+    const int N = s.N;
+    s.G = 0;
+    s.pc = s.vc = s.ac = 0;
+    if (N == 0) return;
+    double4* st = (double4*)stage(sizeof(double4) * (size_t)N * 2 + sizeof(double) * N);
+    if (!st) return;
+    double4* sp = st;
+    double4* sv = st + N;
+    double* sm = (double*)(st + 2 * (size_t)N);
+    for (int i = 0; i < N; ++i) {
+        sp[i] = make_double4(s.h_pos[3 * i], s.h_pos[3 * i + 1], s.h_pos[3 * i + 2], 0.0);
+        sv[i] = make_double4(s.h_vel[3 * i], s.h_vel[3 * i + 1], s.h_vel[3 * i + 2], 0.0);
+        sm[i] = s.h_mass[i];
+    }
+    TMD_CUDA(cudaMemcpyAsync(s.pos.b[0], sp, sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(s.vel.b[0], sv, sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(s.mass.b[0], sm, sizeof(double) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemsetAsync(s.frc.b[0], 0, sizeof(double4) * N, s.stream));
+    TMD_CUDA(cudaMemsetAsync(s.frc32, 0, sizeof(float4) * N, s.stream));
+    k_iota<<<(N + 255) / 256, 256, 0, s.stream>>>(s.ref.b[0], s.slot_of_ref, s.img.b[0], N);
+    launched(K_MISC);
+    // the staging area is reused by later calls: wait for the copies
+    sync_stream(s);
+}
+
+// core/grid.impala:369-374: device -> host mirror, scattered to reference order
+void md_copy_data_from_accelerator(void) {
+    State& s = g_state;
+    if (!require_alive("md_copy_data_from_accelerator")) return;
+    Snapshot sn;
+    snapshot(s, sn);
+    const int NA = s.N + s.G;
+    s.h_mass.assign(NA, 0.0);
+    s.h_pos.assign((size_t)NA * 3, 0.0);
+    s.h_vel.assign((size_t)NA * 3, 0.0);
+    s.h_frc.assign((size_t)NA * 3, 0.0);
+    for (int slot = 0; slot < NA; ++slot) {
+        const int r = sn.ref[slot];
+        if (r < 0 || r >= NA) continue;
+        s.h_mass[r] = sn.mass[slot];
+        s.h_pos[3 * r] = sn.pos[slot].x;
+        s.h_pos[3 * r + 1] = sn.pos[slot].y;
+        s.h_pos[3 * r + 2] = sn.pos[slot].z;
+        if (r < s.N || s.dem_fixed) {
+            s.h_vel[3 * r] = sn.vel[slot].x;
+            s.h_vel[3 * r + 1] = sn.vel[slot].y;
+            s.h_vel[3 * r + 2] = sn.vel[slot].z;
+        }
+        if (r < s.N) {
+            if (s.precision == 1) {
+                s.h_frc[3 * r] = sn.frc32[slot].x;
+                s.h_frc[3 * r + 1] = sn.frc32[slot].y;
+                s.h_frc[3 * r + 2] = sn.frc32[slot].z;
+            } else {
+                s.h_frc[3 * r] = sn.frc[slot].x;
+                s.h_frc[3 * r + 1] = sn.frc[slot].y;
+                s.h_frc[3 * r + 2] = sn.frc[slot].z;
+            }
+        }
+    }
+}
+
+void md_exchange_particles(void) {  // comm/comm.impala:392-525: no remote ranks in one process
+    if (require_alive("md_exchange_particles")) flush_all(g_state);
+}
+
+void md_enforce_pbc(void) {
+    State& s = g_state;
+    if (!require_alive("md_enforce_pbc")) return;
+    flush_all(s);
+    phase_mark(PH_OTHER);
+    run_enforce_pbc(s);
+}
+
+void md_borders(void) {
+    State& s = g_state;
+    if (!require_alive("md_borders")) return;
+    flush_all(s);
+    phase_mark(PH_COMM);
+    run_borders(s);
+}
+
+void md_distribute_particles(void) {
+    State& s = g_state;
+    if (!require_alive("md_distribute_particles")) return;
+    flush_all(s);
+    phase_mark(PH_OTHER);
+    run_distribute(s);
+}
+
+void md_assemble_neighborlists(bool half, double cutoff) {
+    State& s = g_state;
+    if (!require_alive("md_assemble_neighborlists")) return;
+    flush_all(s);
+    phase_mark(PH_NEIGH);
+    run_build_lists(s, half, cutoff);
+}
+
+void md_initial_integration(double dt) {
+    State& s = g_state;
+    if (!require_alive("md_initial_integration")) return;
+    flush_all(s);
+    s.pend_init = true;
+    s.pend_dt = dt;
+}
+
+void md_synchronize_ghost_layer(void) {
+    State& s = g_state;
+    if (!require_alive("md_synchronize_ghost_layer")) return;
+    flush_force(s);
+    phase_mark(PH_COMM);
+    if (s.pend_init) {
+        s.pend_init = false;
+        run_integrate(s, s.pend_dt, true);
+    } else {
+        run_ghost_sync(s);
+    }
+}
+
+void md_compute_lennard_jones(bool half, double rc, double eps, double sigma) {
+    State& s = g_state;
+    if (!require_alive("md_compute_lennard_jones")) return;
+    flush_all(s);
+    PendingForce p;
+    p.valid = true;
+    p.dem = false;
+    p.half = half;
+    p.rc = rc;
+    p.eps = eps;
+    p.sigma = sigma;
+    s.pend_force = p;
+    s.last_rc = rc;
+    s.last_eps = eps;
+    s.last_sigma = sigma;
+}
+
+void md_compute_dem(bool half, double rc, double damping_n, double damping_t, double stiffness, double friction) {
+    State& s = g_state;
+    if (!require_alive("md_compute_dem")) return;
+    flush_all(s);
+    PendingForce p;
+    p.valid = true;
+    p.dem = true;
+    p.half = half;
+    p.rc = rc;
+    p.dn = damping_n;
+    p.dt_ = damping_t;
+    p.k = stiffness;
+    p.mu = friction;
+    s.pend_force = p;
+}
+
+void md_final_integration(double dt) {
+    State& s = g_state;
+    if (!require_alive("md_final_integration")) return;
+    flush_init(s);
+    phase_mark(PH_FORCE);
+    if (s.pend_force.valid) {
+        PendingForce p = s.pend_force;
+        s.pend_force.valid = false;
+        if (!p.dem && !p.half) {
+            launch_force(s, p, true, dt);
+            return;
+        }
+        launch_force(s, p, false, 0.0);
+    }
+    run_final(s, dt);
+}
+
+// core/grid.impala:497-513 (host mirror)
+int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
+    State& s = g_state;
+    if (!require_alive("md_write_grid_data_to_arrays")) return 0;
+    flush_all(s);
+    for (int i = 0; i < s.N && (size_t)3 * i + 2 < s.h_pos.size(); ++i) {
+        m[i] = s.h_mass[i];
+        x[i] = Vector3D{s.h_pos[3 * i], s.h_pos[3 * i + 1], s.h_pos[3 * i + 2]};
+        v[i] = Vector3D{s.h_vel[3 * i], s.h_vel[3 * i + 1], s.h_vel[3 * i + 2]};
+        f[i] = Vector3D{s.h_frc[3 * i], s.h_frc[3 * i + 1], s.h_frc[3 * i + 2]};
+    }
+    return s.N;
+}
+
+// core/grid.impala:515-532: returns nparticles, as the reference does
+int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
+    State& s = g_state;
+    if (!require_alive("md_write_grid_ghost_data_to_arrays")) return 0;
+    flush_all(s);
+    const size_t have = s.h_mass.size();
+    for (int g = 0; g < s.G && (size_t)(s.N + g) < have; ++g) {
+        const size_t p = (size_t)s.N + g;
+        m[g] = s.h_mass[p];
+        x[g] = Vector3D{s.h_pos[3 * p], s.h_pos[3 * p + 1], s.h_pos[3 * p + 2]};
+        v[g] = Vector3D{s.h_vel[3 * p], s.h_vel[3 * p + 1], s.h_vel[3 * p + 2]};
+        f[g] = Vector3D{s.h_frc[3 * p], s.h_frc[3 * p + 1], s.h_frc[3 * p + 2]};
+    }
+    return s.N;
+}
+
+// core/grid.impala:534-560
+int md_write_grid_aabb_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
+    State& s = g_state;
+    const Geometry& g = s.geo;
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j)
+            for (int k = 0; k < 2; ++k) {
+                int idx = k * 4 + j * 2 + i;
+                m[idx] = 0.0;
+                x[idx] = Vector3D{i == 0 ? g.aabb_lo[0] : g.aabb_hi[0], j == 0 ? g.aabb_lo[1] : g.aabb_hi[1],
+                                  k == 0 ? g.aabb_lo[2] : g.aabb_hi[2]};
+                v[idx] = Vector3D{0.0, 0.0, 0.0};
+                f[idx] = Vector3D{0.0, 0.0, 0.0};
+            }
+    return s.N;
+}
+
+void md_deallocate_grid(void) {
+    State& s = g_state;
+    if (s.alive) {
+        flush_all(s);
+        sync_stream(s);
+    }
+    fold_prof(true);
+    phase_reset();
+    free_all(s);
+    s.alive = false;
+    s.N = s.G = 0;
+    s.capA = 0;
+}
+
+// core/runtime.impala:146-156 (host mirror)
+void md_print_grid(void) {
+    State& s = g_state;
+    for (int i = 0; i < s.N; ++i) {
+        std::printf("0> pos_local: ");
+        print_g(s.h_pos[3 * i]); std::printf(", "); print_g(s.h_pos[3 * i + 1]); std::printf(", ");
+        print_g(s.h_pos[3 * i + 2]); std::printf("\n");
+    }
+    for (int i = 0; i < s.N; ++i) {
+        std::printf("0> vel_local: ");
+        print_g(s.h_vel[3 * i]); std::printf(", "); print_g(s.h_vel[3 * i + 1]); std::printf(", ");
+        print_g(s.h_vel[3 * i + 2]); std::printf("\n");
+    }
+    std::fflush(stdout);
+}
+
+void md_print_ghost(void) {
+    State& s = g_state;
+    const size_t have = s.h_mass.size();
+    for (int i = s.N; i < s.N + s.G && (size_t)i < have; ++i) {
+        std::printf("0> pos_ghost: ");
+        print_g(s.h_pos[3 * i]); std::printf(", "); print_g(s.h_pos[3 * i + 1]); std::printf(", ");
+        print_g(s.h_pos[3 * i + 2]); std::printf("\n");
+    }
+    for (int i = s.N; i < s.N + s.G && (size_t)i < have; ++i) {
+        std::printf("0> vel_ghost: ");
+        print_g(s.h_vel[3 * i]); std::printf(", "); print_g(s.h_vel[3 * i + 1]); std::printf(", ");
+        print_g(s.h_vel[3 * i + 2]); std::printf("\n");
+    }
+    std::fflush(stdout);
+}
+
+void md_mpi_initialize(void) {}
+void md_mpi_finalize(void) {}
+void md_barrier(void) {  // no other ranks: wait for this rank's device work
+    State& s = g_state;
+    if (s.alive) {
+        flush_all(s);
+        sync_stream(s);
+    }
+}
+int md_get_world_size(void) { return 1; }
+int md_get_world_rank(void) { return 0; }
+int md_get_number_of_particles(void) { return g_state.N; }
+int md_get_number_of_ghost_particles(void) { return g_state.G; }
+
+// comm/comm.impala:254-331 with one rank
+void md_get_node_bounding_box(double const* aabb, double (*rank)[6]) {
+    for (int d = 0; d < 3; ++d) {
+        double len = (aabb[2 * d + 1] - aabb[2 * d]) / 1.0;
+        double lo = aabb[2 * d] + len * 0.0;
+        (*rank)[2 * d] = lo;
+        (*rank)[2 * d + 1] = lo + len;
+    }
+}
+
+// load balancing / multi-process entry points (out of scope on one GPU)
+void md_rescale_grid(double const* aabb) {
+    (void)aabb;
+    set_error(MD_ERR_UNSUPPORTED, "md_rescale_grid: load balancing is not supported on one GPU");
+}
+double md_get_send_buffer_value(int i) {
+    (void)i;
+    return 0.0;
+}
+void md_set_recv_buffer_value(int i, double v) {
+    (void)i;
+    (void)v;
+}
+void md_resize_recv_buffer_capacity(int c) { (void)c; }
+int md_serialize_particles(double const* aabb) {
+    (void)aabb;
+    set_error(MD_ERR_UNSUPPORTED, "md_serialize_particles: load balancing is not supported on one GPU");
+    return 0;
+}
+void md_deserialize_particles(int n) {
+    (void)n;
+    set_error(MD_ERR_UNSUPPORTED, "md_deserialize_particles: load balancing is not supported on one GPU");
+}
+void md_update_neighborhood(int nranks, int total, int const* ranks, int const* naabbs, double const* aabbs) {
+    (void)nranks; (void)total; (void)ranks; (void)naabbs; (void)aabbs;
+}
+
+// core/runtime.impala:72-95: locals / ghosts inside the box
+void md_compute_boundary_weights(double xmin, double xmax, double ymin, double ymax, double zmin, double zmax,
+                                 unsigned long int* comp_w, unsigned long int* comm_w) {
+    State& s = g_state;
+    *comp_w = 0;
+    *comm_w = 0;
+    if (!s.alive) return;
+    Snapshot sn;
+    snapshot(s, sn);
+    auto inside = [&](const double4& p) {
+        return p.x >= xmin && p.x <= xmax && p.y >= ymin && p.y <= ymax && p.z >= zmin && p.z <= zmax;
+    };
+    for (int slot = 0; slot < s.N + s.G; ++slot) {
+        if (!inside(sn.pos[slot])) continue;
+        if (sn.ref[slot] < s.N) (*comp_w)++;
+        else (*comm_w)++;
+    }
+}
+
+// core/runtime.impala:280-296
+void md_report_iterations(void) {
+    State& s = g_state;
+    long long total = 0;
+    if (s.alive) {
+        flush_all(s);
+        std::vector<int> n(s.N);
+        if (s.N) {
+            TMD_CUDA(cudaMemcpyAsync(n.data(), s.nbn, sizeof(int) * s.N, cudaMemcpyDeviceToHost, s.stream));
+            sync_stream(s);
+        }
+        if (s.lists_valid)
+            for (int v : n) total += v;
+    }
+    s.force_iters = total;
+    std::printf("ForceIters RsqIters IntegrationIters\n");
+    std::printf("%lld %lld %lld \n", s.force_iters, s.rsq_iters, s.integration_iters);
+    std::fflush(stdout);
+}
+
+// core/runtime.impala:298-316 (temperature from the host mirror)
+void md_report_particles(void) {
+    State& s = g_state;
+    if (s.alive) flush_all(s);
+    std::printf("# Local # Ghost Temp\n");
+    std::printf("%d %d ", s.N, s.G);
+    print_g(host_temperature(s));
+    std::printf("\n");
+    std::fflush(stdout);
+}
+
+// core/runtime.impala:318-337
+void md_report_time(double total, double force, double neigh, double comm, double lb, double other) {
+    std::printf("Total Force Neigh Comm Balance Other\n");
+    double v[6] = {total, force, neigh, comm, lb, other};
+    for (double x : v) {
+        print_g(x);
+        std::printf(" ");
+    }
+    std::printf("\n");
+    std::fflush(stdout);
+}
+
+// ---- extensions ---------------------------------------------------------------
+void md_set_precision(int mode) {
+    State& s = g_state;
+    mode = mode ? 1 : 0;
+    if (s.alive && mode != s.precision) {
+        flush_all(s);
+        const int NA = s.N + s.G;
+        if (NA > 0) {
+            k_convert_forces<<<(NA + 255) / 256, 256, 0, s.stream>>>(s.frc.b[s.ac], s.frc32, NA, mode);
+            launched(K_MISC);
+        }
+        s.precision = mode;
+        if (mode == 1) run_refresh_pos32(s);
+    }
+    s.precision = mode;
+}
+void md_set_ghost_mode(int exact) {
+    if (g_state.alive) flush_all(g_state);
+    g_state.ghost_exact = exact ? 1 : 0;
+}
+void md_set_dem_model(int fixed, double radius) {
+    if (g_state.alive) flush_all(g_state);
+    g_state.dem_fixed = fixed ? 1 : 0;
+    g_state.dem_radius = radius;
+}
+void md_set_thermo(int enable) {
+    if (g_state.alive) flush_all(g_state);
+    g_state.thermo = enable ? 1 : 0;
+}
+int md_get_thermo(double* out) {
+    State& s = g_state;
+    if (!require_alive("md_get_thermo")) return -1;
+    flush_all(s);
+    TMD_CUDA(cudaMemcpyAsync(out, s.thermo_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    sync_stream(s);
+    s.rsq_iters = (long long)out[2];
+    return 0;
+}
+void md_synchronize(void) {
+    if (g_state.alive) {
+        flush_all(g_state);
+        sync_stream(g_state);
+    }
+}
+void md_get_phase_times(double* out) {
+    if (g_state.alive) flush_all(g_state);
+    phase_times(out);
+}
+void md_profile_enable(int mask) {
+    if (g_state.alive) flush_all(g_state);
+    prof_mask = mask;
+}
+int md_profile_count(void) { return K_COUNT; }
+const char* md_profile_name(int id) { return kernel_name(id); }
+int md_profile_get(int id, long long* launches, double* total_ms) {
+    if (id < 0 || id >= K_COUNT) return -1;
+    if (g_state.alive) flush_all(g_state);
+    fold_prof(true);
+    *launches = prof_launch[id];
+    *total_ms = prof_ms[id];
+    return 0;
+}
+void md_profile_reset(void) { prof_reset(); }
+long long md_kernel_launches(void) { return g_state.launches; }
+long long md_device_bytes(void) { return g_state.dev_bytes; }
+
+int md_get_neighbor_lists(int* sizes, int* lists, int capacity) {
+    State& s = g_state;
+    if (!require_alive("md_get_neighbor_lists")) return -1;
+    flush_all(s);
+    const int N = s.N, NA = s.N + s.G;
+    std::vector<int> n(N), ref(NA);
+    std::vector<uint32_t> l((size_t)s.nb_cap * s.nb_stride);
+    TMD_CUDA(cudaMemcpyAsync(n.data(), s.nbn, sizeof(int) * N, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(ref.data(), s.ref.b[s.ac], sizeof(int) * NA, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(l.data(), s.nbl, sizeof(uint32_t) * l.size(), cudaMemcpyDeviceToHost, s.stream));
+    sync_stream(s);
+    int mx = 0;
+    for (int slot = 0; slot < N; ++slot) {
+        const int r = ref[slot];
+        sizes[r] = n[slot];
+        mx = std::max(mx, n[slot]);
+        for (int k = 0; k < n[slot] && k < capacity && k < s.nb_cap; ++k)
+            lists[(size_t)r * capacity + k] = ref[l[(size_t)k * s.nb_stride + slot] >> kCodeBits];
+    }
+    return mx;
+}
+
+int md_get_ghost_info(int* src, int* pbc, int* root, int* tshift) {
+    State& s = g_state;
+    if (!require_alive("md_get_ghost_info")) return -1;
+    flush_all(s);
+    const int G = s.G;
+    std::vector<int> a(G), b(G), c(G);
+    if (G) {
+        TMD_CUDA(cudaMemcpyAsync(a.data(), s.bsrc_ref, sizeof(int) * G, cudaMemcpyDeviceToHost, s.stream));
+        TMD_CUDA(cudaMemcpyAsync(b.data(), s.broot_ref, sizeof(int) * G, cudaMemcpyDeviceToHost, s.stream));
+        TMD_CUDA(cudaMemcpyAsync(c.data(), s.bcode, sizeof(int) * G, cudaMemcpyDeviceToHost, s.stream));
+        sync_stream(s);
+    }
+    for (int g = 0; g < G; ++g) {
+        src[g] = a[g];
+        root[g] = b[g];
+        for (int d = 0; d < 3; ++d) {
+            pbc[3 * g + d] = ((c[g] >> (2 * d)) & 3) - 1;
+            tshift[3 * g + d] = ((c[g] >> (8 + 2 * d)) & 3) - 1;
+        }
+    }
+    return G;
+}
+
+int md_get_state(double* pos, double* vel, double* frc) {
+    State& s = g_state;
+    if (!require_alive("md_get_state")) return -1;
+    Snapshot sn;
+    snapshot(s, sn);
+    for (int slot = 0; slot < s.N + s.G; ++slot) {
+        const int r = sn.ref[slot];
+        if (pos) {
+            pos[3 * r] = sn.pos[slot].x;
+            pos[3 * r + 1] = sn.pos[slot].y;
+            pos[3 * r + 2] = sn.pos[slot].z;
+        }
+        if (r >= s.N) continue;
+        if (vel) {
+            vel[3 * r] = sn.vel[slot].x;
+            vel[3 * r + 1] = sn.vel[slot].y;
+            vel[3 * r + 2] = sn.vel[slot].z;
+        }
+        if (frc) {
+            if (s.precision == 1) {
+                frc[3 * r] = sn.frc32[slot].x;
+                frc[3 * r + 1] = sn.frc32[slot].y;
+                frc[3 * r + 2] = sn.frc32[slot].z;
+            } else {
+                frc[3 * r] = sn.frc[slot].x;
+                frc[3 * r + 1] = sn.frc[slot].y;
+                frc[3 * r + 2] = sn.frc[slot].z;
+            }
+        }
+    }
+    return s.N + s.G;
+}
+
+static int set_local_vec(const double* in, bool is_pos) {
+    State& s = g_state;
+    if (!require_alive("md_set_positions")) return -1;
+    flush_all(s);
+    const int N = s.N;
+    std::vector<int> sor(N);
+    std::vector<double4> buf(N);
+    double4* dst = is_pos ? s.pos.b[s.pc] : s.vel.b[s.vc];
+    TMD_CUDA(cudaMemcpyAsync(sor.data(), s.slot_of_ref, sizeof(int) * N, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(buf.data(), dst, sizeof(double4) * N, cudaMemcpyDeviceToHost, s.stream));
+    sync_stream(s);
+    for (int r = 0; r < N; ++r) {
+        double4& q = buf[sor[r]];
+        q.x = in[3 * r];
+        q.y = in[3 * r + 1];
+        q.z = in[3 * r + 2];
+    }
+    TMD_CUDA(cudaMemcpyAsync(dst, buf.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
+    sync_stream(s);
+    if (is_pos && s.precision == 1) run_refresh_pos32(s);
+    return 0;
+}
+int md_set_positions(double const* pos) { return set_local_vec(pos, true); }
+int md_set_velocities(double const* vel) { return set_local_vec(vel, false); }
+
+int md_get_cell_sizes(int* out, int ncells) {
+    State& s = g_state;
+    if (!require_alive("md_get_cell_sizes")) return -1;
+    flush_all(s);
+    const int nc = s.geo.ncells;
+    std::vector<int> c(2 * (nc + 1));
+    TMD_CUDA(cudaMemcpyAsync(c.data(), s.cnt, sizeof(int) * c.size(), cudaMemcpyDeviceToHost, s.stream));
+    sync_stream(s);
+    for (int k = 0; k < nc && k < ncells; ++k) out[k] = c[k] + c[nc + 1 + k];
+    return nc;
+}
+
+int md_get_grid_info(int* out) {
+    State& s = g_state;
+    out[0] = s.geo.nx;
+    out[1] = s.geo.ny;
+    out[2] = s.geo.nz;
+    out[3] = s.geo.ncells;
+    out[4] = s.N;
+    out[5] = s.G;
+    out[6] = s.nb_cap;
+    out[7] = s.nb_stride;
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,709 @@
+// k_neigh.cu -- reneighbour kernels of the tinyMD B200 timestep:
+//   * periodic wrap of locals        (core/compute.impala:196-200, comm/comm.impala:152-162)
+//   * ghost generation (borders)     (comm/comm.impala:105-127, 528-642, 723-734; comm/lb.impala:88-100)
+//   * cell binning as a counting sort that reorders the device arrays by cell
+//                                    (core/grid.impala:280-321, 406-426)
+//   * neighbour-list build, one warp per cell, ballot/popc compaction
+//                                    (core/neighborlist.impala:1-78)
+//
+// Ghost order.  The reference runs six passes (x+, x-, y+, y-, z+, z-); a
+// pass scans locals then all earlier ghosts in order and appends the ones
+// within one cell of the face, shifted by one box length.  A ghost is
+// therefore identified by its root local r and its pass combination
+// (ex, ey, ez) with e in {0 none, 1 plus pass, 2 minus pass}, and the
+// reference appends them grouped by base-3 type index ez*9 + ey*3 + ex - 1,
+// in increasing r inside a type.  The kernels below compute that order
+// directly: one mask per local, per-type counts, one exclusive scan, emit.
+//
+// In-cell order.  The reference fills cells sequentially by particle index,
+// so a cell lists its locals in input order, then its ghosts in ghost order.
+// The counting sort here ranks each cell's members by that reference index,
+// which makes list order -- and hence FP64 force summation order -- equal to
+// the reference's.
+
+#include <cstdio>
+
+#include "md_common.cuh"
+#include "md_state.h"
+
+namespace tmd {
+
+namespace {
+
+struct GeoArgs {
+    double wlo[3], whi[3], alo[3], ahi[3], len[3];
+    double spacing;
+    int nx, ny, nz, ncells;
+    double rb_h;
+};
+
+GeoArgs geo_args(const Geometry& g) {
+    GeoArgs a;
+    for (int d = 0; d < 3; ++d) {
+        a.wlo[d] = g.world_lo[d];
+        a.whi[d] = g.world_hi[d];
+        a.alo[d] = g.aabb_lo[d];
+        a.ahi[d] = g.aabb_hi[d];
+        a.len[d] = g.len[d];
+    }
+    a.spacing = g.spacing;
+    a.nx = g.nx;
+    a.ny = g.ny;
+    a.nz = g.nz;
+    a.ncells = g.ncells;
+    a.rb_h = g.rb_h;
+    return a;
+}
+
+__device__ __forceinline__ double comp(const double4& p, int d) { return d == 0 ? p.x : (d == 1 ? p.y : p.z); }
+
+// core/grid.impala:406-411 and 419-426: floor per axis, flattened, with only
+// the global range check.  Returns ncells when outside.
+__device__ __forceinline__ int flat_cell(const double4& p, const GeoArgs& a) {
+    int i = (int)floor(ddiv(dsub(p.x, a.alo[0]), a.spacing));
+    int j = (int)floor(ddiv(dsub(p.y, a.alo[1]), a.spacing));
+    int k = (int)floor(ddiv(dsub(p.z, a.alo[2]), a.spacing));
+    int c = (k * a.ny + j) * a.nx + i;
+    return (c >= 0 && c < a.ncells) ? c : a.ncells;
+}
+
+__device__ __forceinline__ int rebase_cell(const double4& p, const GeoArgs& a) {
+    int i = (int)floor((p.x - a.alo[0]) / a.rb_h);
+    int j = (int)floor((p.y - a.alo[1]) / a.rb_h);
+    int k = (int)floor((p.z - a.alo[2]) / a.rb_h);
+    return pack3(i, j, k);
+}
+
+}  // namespace
+
+// ---- periodic wrap ---------------------------------------------------------
+// comm/comm.impala:152-162: one wrap per axis with strict comparisons against
+// the world box.  img counts wraps so the adjoint can unwrap displacements.
+__global__ void k_enforce_pbc(double4* __restrict__ pos, int* __restrict__ img, int N, GeoArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double4 p = pos[i];
+    double c[3] = {p.x, p.y, p.z};
+    int im = img[i];
+    int w[3] = {unpack_axis(im, 0), unpack_axis(im, 1), unpack_axis(im, 2)};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double v = comp(p, d);
+        if (v < a.wlo[d]) { c[d] = dadd(c[d], a.len[d]); w[d] -= 1; }
+        if (v > a.whi[d]) { c[d] = dsub(c[d], a.len[d]); w[d] += 1; }
+    }
+    pos[i] = make_double4(c[0], c[1], c[2], p.w);
+    img[i] = pack3(w[0], w[1], w[2]);
+}
+
+// ---- borders ---------------------------------------------------------------
+// Mask of the 26 ghost types of one local (bit t = ez*9 + ey*3 + ex - 1) in
+// bits 0-25 and the six periodic flags of its passes in bits 26-31
+// (x+, x-, y+, y-, z+, z-): flag set means the pass shifts that axis.
+__device__ __forceinline__ unsigned border_mask(const double4& p, const GeoArgs& a) {
+    const double dsp = dmul(a.spacing, 2.0);
+    unsigned has[3] = {0, 0, 0};  // bit0 plus pass, bit1 minus pass
+    unsigned flags = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double v = comp(p, d);
+        // comm/comm.impala:116-127 (grid.aabb is the extended rank box)
+        if (v > dsub(a.ahi[d], dsp)) has[d] |= 1u;
+        if (v < dadd(a.alo[d], dsp)) has[d] |= 2u;
+        // comm/lb.impala:88-100 with the pass direction
+        if (v > dsub(a.whi[d], a.spacing)) flags |= 1u << (2 * d);
+        if (v < dadd(a.wlo[d], a.spacing)) flags |= 1u << (2 * d + 1);
+    }
+    unsigned mask = 0;
+    for (int ez = 0; ez < 3; ++ez) {
+        if (ez && !(has[2] & (1u << (ez - 1)))) continue;
+        for (int ey = 0; ey < 3; ++ey) {
+            if (ey && !(has[1] & (1u << (ey - 1)))) continue;
+            for (int ex = 0; ex < 3; ++ex) {
+                if (ex && !(has[0] & (1u << (ex - 1)))) continue;
+                int t = ez * 9 + ey * 3 + ex;
+                if (t) mask |= 1u << (t - 1);
+            }
+        }
+    }
+    return mask | (flags << 26);
+}
+
+// Pass 1: masks in reference order and per-block per-type counts [26][nblk].
+__global__ void k_border_count(const double4* __restrict__ pos, const int* __restrict__ slot_of_ref,
+                               unsigned* __restrict__ bmask, int* __restrict__ bcount, int N, int nblk, GeoArgs a) {
+    __shared__ int wc[8][26];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned m = 0;
+    if (r < N) {
+        m = border_mask(pos[slot_of_ref[r]], a);
+        bmask[r] = m;
+    }
+    for (int t = 0; t < 26; ++t) {
+        unsigned b = __ballot_sync(0xffffffffu, (m >> t) & 1u);
+        if (lane == 0) wc[wid][t] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < 26) {
+        int s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += wc[w][threadIdx.x];
+        bcount[threadIdx.x * nblk + blockIdx.x] = s;
+    }
+}
+
+// Pass 2 (after an exclusive scan of bcount into boff): writes every ghost at
+// slot N + g, g its reference ghost index, with its source / root links.
+__global__ void k_border_emit(double4* __restrict__ pos, double4* __restrict__ vel, double4* __restrict__ frc,
+                              double* __restrict__ mass, int* __restrict__ ref, int* __restrict__ slot_of_ref,
+                              const unsigned* __restrict__ bmask, const int* __restrict__ boff,
+                              int* __restrict__ gsrc, int* __restrict__ groot, int* __restrict__ gcode,
+                              int* __restrict__ bsrc_ref, int* __restrict__ broot_ref, int* __restrict__ bcode,
+                              int N, int nblk, int capA, GeoArgs a, int sync_vel) {
+    __shared__ int wpre[8][26];
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned m = r < N ? bmask[r] : 0u;
+    const unsigned lt = lanemask_lt();
+    int rank[26];
+    for (int t = 0; t < 26; ++t) {
+        unsigned b = __ballot_sync(0xffffffffu, (m >> t) & 1u);
+        rank[t] = __popc(b & lt);
+        if (lane == 0) wpre[wid][t] = __popc(b);
+    }
+    __syncthreads();
+    if (threadIdx.x < 26) {  // exclusive prefix over warps, per type
+        int s = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            int c = wpre[w][threadIdx.x];
+            wpre[w][threadIdx.x] = s;
+            s += c;
+        }
+    }
+    __syncthreads();
+    if (r >= N || (m & 0x03ffffffu) == 0) return;
+    const int s_root = slot_of_ref[r];
+    const double4 p = pos[s_root];
+    const double mroot = mass[s_root];
+    const double4 vroot = vel[s_root];
+    const unsigned flags = m >> 26;
+    int gidx[26];
+    for (int t = 0; t < 26; ++t) gidx[t] = ((m >> t) & 1u) ? boff[t * nblk + blockIdx.x] + wpre[wid][t] + rank[t] : -1;
+    for (int t = 0; t < 26; ++t) {
+        if (!((m >> t) & 1u)) continue;
+        const int g = gidx[t];
+        const int slot = N + g;
+        if (slot >= capA) continue;  // the host grows the arrays and redoes the pass
+        const int tt = t + 1;
+        const int e[3] = {tt % 3, (tt / 3) % 3, tt / 9};
+        int last = e[2] ? 2 : (e[1] ? 1 : 0);
+        double c[3] = {p.x, p.y, p.z};
+        int tot[3] = {0, 0, 0};
+        int lastsh = 0;
+        for (int d = 0; d < 3; ++d) {
+            if (!e[d]) continue;
+            // plus pass shifts by -1 when the flag holds, minus pass by +1
+            int sh = 0;
+            if (e[d] == 1 && (flags & (1u << (2 * d)))) sh = -1;
+            if (e[d] == 2 && (flags & (1u << (2 * d + 1)))) sh = 1;
+            c[d] = dadd(c[d], dmul(a.len[d], (double)sh));
+            tot[d] = sh;
+            if (d == last) lastsh = sh;
+        }
+        // source of the last pass: the ghost of the same root without the last axis, or the root
+        const int tsrc = tt - e[last] * (last == 0 ? 1 : (last == 1 ? 3 : 9));
+        const int src_ref = tsrc == 0 ? r : N + gidx[tsrc - 1];
+        const int src_slot = tsrc == 0 ? s_root : N + gidx[tsrc - 1];
+        int code = 0;
+        for (int d = 0; d < 3; ++d) {
+            int ls = (d == last) ? lastsh : 0;
+            code |= (ls + 1) << (2 * d);
+            code |= (tot[d] + 1) << (8 + 2 * d);
+        }
+        pos[slot] = make_double4(c[0], c[1], c[2], 0.0);
+        mass[slot] = mroot;
+        frc[slot] = make_double4(0.0, 0.0, 0.0, 0.0);
+        vel[slot] = sync_vel ? vroot : make_double4(0.0, 0.0, 0.0, 0.0);
+        ref[slot] = slot;
+        slot_of_ref[slot] = slot;
+        gsrc[g] = src_slot;
+        groot[g] = s_root;
+        gcode[g] = code;
+        bsrc_ref[g] = src_ref;
+        broot_ref[g] = r;
+        bcode[g] = code;
+    }
+}
+
+// ---- binning (counting sort) -----------------------------------------------
+// cnt / cstart layout: [0, ncells] locals per cell (index ncells = outside
+// the grid), [ncells+1, 2*ncells+1] ghosts per cell.
+__global__ void k_bin_count(const double4* __restrict__ pos, int* __restrict__ cnt, int* __restrict__ bin_cell,
+                            int* __restrict__ bin_rank, DevStatus* st, int N, int NA, GeoArgs a) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= NA) return;
+    int c = flat_cell(pos[s], a);
+    if (c == a.ncells) atomicAdd(s < N ? &st->out_local : &st->out_ghost, 1);
+    int seg = s < N ? c : (a.ncells + 1) + c;
+    bin_cell[s] = c;
+    bin_rank[s] = atomicAdd(&cnt[seg], 1);
+}
+
+__global__ void k_bin_scatter(const int* __restrict__ ref, const int* __restrict__ bin_cell,
+                              const int* __restrict__ bin_rank, const int* __restrict__ cstart,
+                              int* __restrict__ tmp_key, int* __restrict__ tmp_src, int N, int NA, int ncells) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= NA) return;
+    int c = bin_cell[s];
+    int seg = s < N ? c : (ncells + 1) + c;
+    int p = cstart[seg] + bin_rank[s];
+    tmp_key[p] = ref[s];
+    tmp_src[p] = s;
+}
+
+// One warp per segment: rank members by reference index (keys are unique).
+__global__ void k_bin_rank(const int* __restrict__ cstart, const int* __restrict__ tmp_key,
+                           const int* __restrict__ tmp_src, int* __restrict__ perm, int nseg) {
+    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (w >= nseg) return;
+    int a = cstart[w], b = cstart[w + 1];
+    for (int e = a + lane; e < b; e += 32) {
+        int key = tmp_key[e];
+        int rank = 0;
+        for (int f = a; f < b; ++f) rank += tmp_key[f] < key;
+        perm[a + rank] = tmp_src[e];
+    }
+}
+
+__global__ void k_permute(const int* __restrict__ perm, const double4* __restrict__ pos_o, double4* __restrict__ pos_n,
+                          const double4* __restrict__ vel_o, double4* __restrict__ vel_n,
+                          const double4* __restrict__ frc_o, double4* __restrict__ frc_n,
+                          const double* __restrict__ mass_o, double* __restrict__ mass_n,
+                          const int* __restrict__ ref_o, int* __restrict__ ref_n, const int* __restrict__ img_o,
+                          int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rbk,
+                          float4* __restrict__ pos32, int NA, int N, GeoArgs a, int mixed) {
+    int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= NA) return;
+    int o = perm[n];
+    double4 p = pos_o[o];
+    pos_n[n] = p;
+    vel_n[n] = vel_o[o];
+    frc_n[n] = frc_o[o];
+    mass_n[n] = mass_o[o];
+    int r = ref_o[o];
+    ref_n[n] = r;
+    if (n < N) img_n[n] = img_o[o];
+    slot_of_ref[r] = n;
+    int k = rebase_cell(p, a);
+    rbk[n] = k;
+    if (mixed) pos32[n] = rebased32(p, k, a.alo, a.rb_h);
+}
+
+__global__ void k_ghost_links(const int* __restrict__ ref, const int* __restrict__ slot_of_ref,
+                              const int* __restrict__ bsrc_ref, const int* __restrict__ broot_ref,
+                              const int* __restrict__ bcode, int* __restrict__ gsrc, int* __restrict__ groot,
+                              int* __restrict__ gcode, int N, int G) {
+    int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= G) return;
+    int g = ref[N + h] - N;
+    gsrc[h] = slot_of_ref[bsrc_ref[g]];
+    groot[h] = slot_of_ref[broot_ref[g]];
+    gcode[h] = bcode[g];
+}
+
+// ---- neighbour lists ---------------------------------------------------------
+constexpr int kNlWarps = 4;    // warps (cells) per block
+constexpr int kTile = 128;     // staged candidates per warp and tile
+constexpr int kHomeMax = 64;   // home atoms handled per pass over the candidates
+
+struct NlArgs {
+    double cut2;     // cutoff^2 (FP64, the reference's membership test)
+    float lo2, hi2;  // FP32 prefilter: certainly inside below lo2, certainly outside above hi2
+    int nbcap, stride, N, ncells, nx, nxy;
+    double alo[3], spacing;
+};
+
+template <bool HALF>
+__global__ void __launch_bounds__(kNlWarps * 32)
+k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
+             const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl,
+             DevStatus* st, NlArgs a) {
+    __shared__ float4 s_cpos[kNlWarps][kTile];  // candidate relative position, w = slot bits
+    __shared__ int s_cref[kNlWarps][kTile];
+    __shared__ int s_crbk[kNlWarps][kTile];
+    __shared__ float4 s_hpos[kNlWarps][kHomeMax];
+    __shared__ int s_hcnt[kNlWarps][kHomeMax];
+    __shared__ int s_rstart[kNlWarps][54];
+    __shared__ int s_rpre[kNlWarps][55];
+
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kNlWarps + wid;
+    if (c >= a.ncells) return;
+    const int h0 = cstart[c], h1 = cstart[c + 1];
+    if (h0 == h1) return;
+    const unsigned lt = lanemask_lt();
+
+    // 27 stencil cells in the reference order (z, y, x offsets -1..1), each
+    // contributing its locals then its ghosts: 54 ranges
+    int len = 0, start = 0;
+    if (lane < 27) {
+        int oz = lane / 9 - 1, oy = (lane / 3) % 3 - 1, ox = lane % 3 - 1;
+        int nb = c + oz * a.nxy + oy * a.nx + ox;
+        if (nb >= 0 && nb < a.ncells) {
+            start = cstart[nb];
+            len = cstart[nb + 1] - start;
+            int gs = cstart[a.ncells + 1 + nb];
+            s_rstart[wid][2 * lane + 1] = gs;
+            s_rpre[wid][2 * lane + 1] = cstart[a.ncells + 2 + nb] - gs;  // ghost length (temporarily)
+        } else {
+            s_rstart[wid][2 * lane + 1] = 0;
+            s_rpre[wid][2 * lane + 1] = 0;
+        }
+        s_rstart[wid][2 * lane] = start;
+        s_rpre[wid][2 * lane] = len;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        int acc = 0;
+        for (int q = 0; q < 54; ++q) {
+            int l = s_rpre[wid][q];
+            s_rpre[wid][q] = acc;
+            acc += l;
+        }
+        s_rpre[wid][54] = acc;
+    }
+    __syncwarp();
+    const int M = s_rpre[wid][54];
+
+    const int cz = c / a.nxy, cy = (c / a.nx) % (a.nxy / a.nx), cx = c % a.nx;
+    const double ctr[3] = {a.alo[0] + ((double)cx + 0.5) * a.spacing, a.alo[1] + ((double)cy + 0.5) * a.spacing,
+                           a.alo[2] + ((double)cz + 0.5) * a.spacing};
+    int maxcnt = 0;
+
+    for (int hb = h0; hb < h1; hb += kHomeMax) {
+        const int hn = min(kHomeMax, h1 - hb);
+        for (int q = lane; q < hn; q += 32) {
+            double4 p = pos[hb + q];
+            s_hpos[wid][q] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]), (float)(p.z - ctr[2]), 0.0f);
+            s_hcnt[wid][q] = 0;
+        }
+        __syncwarp();
+        for (int t0 = 0; t0 < M; t0 += kTile) {
+            const int tn = min(kTile, M - t0);
+            for (int q = 0; q < 54; ++q) {
+                const int ra = max(s_rpre[wid][q], t0), rb = min(s_rpre[wid][q + 1], t0 + tn);
+                for (int m = ra + lane; m < rb; m += 32) {
+                    const int slot = s_rstart[wid][q] + (m - s_rpre[wid][q]);
+                    double4 p = pos[slot];
+                    s_cpos[wid][m - t0] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]),
+                                                      (float)(p.z - ctr[2]), __int_as_float(slot));
+                    s_cref[wid][m - t0] = HALF ? ref[slot] : 0;
+                    s_crbk[wid][m - t0] = rbk[slot];
+                }
+            }
+            __syncwarp();
+            for (int h = 0; h < hn; ++h) {
+                const int i = hb + h;
+                const float4 hp = s_hpos[wid][h];
+                const int iref = HALF ? ref[i] : 0;
+                const int irbk = rbk[i];
+                int cnt = s_hcnt[wid][h];
+                for (int q0 = 0; q0 < tn; q0 += 32) {
+                    const int q = q0 + lane;
+                    bool pred = false;
+                    int slot = -1;
+                    int code = 0;
+                    if (q < tn) {
+                        const float4 cp = s_cpos[wid][q];
+                        slot = __float_as_int(cp.w);
+                        const float dx = hp.x - cp.x, dy = hp.y - cp.y, dz = hp.z - cp.z;
+                        const float r2 = dx * dx + dy * dy + dz * dz;
+                        bool in = r2 < a.lo2;
+                        if (!in && r2 <= a.hi2) {
+                            // near the cutoff: the reference's exact FP64 test
+                            const double4 pi = pos[i], pj = pos[slot];
+                            in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
+                        }
+                        pred = in && slot != i && (!HALF || s_cref[wid][q] < iref);
+                        if (pred) {
+                            const int cr = s_crbk[wid][q];
+                            int dkx = wrap_diff(unpack_axis(cr, 0), unpack_axis(irbk, 0));
+                            int dky = wrap_diff(unpack_axis(cr, 1), unpack_axis(irbk, 1));
+                            int dkz = wrap_diff(unpack_axis(cr, 2), unpack_axis(irbk, 2));
+                            if (dkx < -1 || dkx > 1 || dky < -1 || dky > 1 || dkz < -1 || dkz > 1) {
+                                atomicAdd(&st->bad_code, 1);
+                                dkx = dky = dkz = 0;
+                            }
+                            code = (dkx + 1) | ((dky + 1) << 2) | ((dkz + 1) << 4);
+                        }
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, pred);
+                    if (pred) {
+                        const int p = cnt + __popc(bal & lt);
+                        if (p < a.nbcap) nbl[(size_t)p * a.stride + i] = ((uint32_t)slot << kCodeBits) | (uint32_t)code;
+                    }
+                    cnt += __popc(bal);
+                }
+                if (lane == 0) s_hcnt[wid][h] = cnt;
+                __syncwarp();
+            }
+            __syncwarp();
+        }
+        for (int q = lane; q < hn; q += 32) {
+            const int n = s_hcnt[wid][q];
+            nbn[hb + q] = n;
+            maxcnt = max(maxcnt, n);
+        }
+        __syncwarp();
+    }
+    maxcnt = warp_max(maxcnt);
+    if (lane == 0) atomicMax(&st->max_nb, maxcnt);
+}
+
+// Locals outside the grid (bucket ncells) get empty lists.
+__global__ void k_clear_lists(int* __restrict__ nbn, int a, int b) {
+    int i = a + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < b) nbn[i] = 0;
+}
+
+// ---- exclusive scan ------------------------------------------------------------
+__device__ __forceinline__ int block_exscan(int v, int* total, int* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = blockDim.x >> 5;
+        int w = lane < nw ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        sh[lane] = w;  // inclusive prefix of warp sums
+    }
+    __syncthreads();
+    int r = x - v + (wid ? sh[wid - 1] : 0);
+    *total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return r;
+}
+
+constexpr int kScanThreads = 1024, kScanItems = 4, kScanBlock = kScanThreads * kScanItems;
+
+// per-block totals of the input
+__global__ void k_scan_sums(const int* __restrict__ in, int* __restrict__ part, int n) {
+    __shared__ int sh[32];
+    int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    int s = 0;
+    for (int k = 0; k < kScanItems; ++k) s += (base + k < n) ? in[base + k] : 0;
+    int tot;
+    block_exscan(s, &tot, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = tot;
+}
+
+// exclusive scan of the block totals in place (one block); part[nb] = grand total
+__global__ void k_scan_part(int* __restrict__ part, int nb) {
+    __shared__ int sh[32];
+    int carry = 0;
+    for (int b0 = 0; b0 < nb; b0 += kScanThreads) {
+        int i = b0 + threadIdx.x;
+        int v = i < nb ? part[i] : 0;
+        int tot;
+        int ex = block_exscan(v, &tot, sh);
+        if (i < nb) part[i] = carry + ex;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[nb] = carry;
+}
+
+__global__ void k_scan_apply(const int* __restrict__ in, int* __restrict__ out, const int* __restrict__ part,
+                             int n, int nb) {
+    __shared__ int sh[32];
+    int base = blockIdx.x * kScanBlock + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = (base + k < n) ? in[base + k] : 0;
+        s += v[k];
+    }
+    int tot;
+    int ex = block_exscan(s, &tot, sh) + part[blockIdx.x];
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = ex;
+        ex += v[k];
+    }
+    if (blockIdx.x == nb - 1 && threadIdx.x == 0) out[n] = part[nb];
+}
+
+// ---- host wrappers ---------------------------------------------------------------
+static inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+void ensure_scan_scratch(State& s, int n) {
+    int nb = nblocks(n, kScanBlock) + 1;
+    if (nb > s.scan_part_cap) {
+        dfree(&s.scan_part);
+        s.scan_part_cap = nb + 64;
+        dalloc(&s.scan_part, s.scan_part_cap);
+    }
+}
+
+// out[0..n-1] = exclusive prefix sums of in, out[n] = total (in != out allowed only)
+void exclusive_scan(State& s, const int* in, int* out, int n) {
+    int nb = nblocks(n, kScanBlock);
+    if (nb < 1) nb = 1;
+    ensure_scan_scratch(s, n);
+    k_scan_sums<<<nb, kScanThreads, 0, s.stream>>>(in, s.scan_part, n);
+    launched(K_SCAN);
+    k_scan_part<<<1, kScanThreads, 0, s.stream>>>(s.scan_part, nb);
+    launched(K_SCAN);
+    k_scan_apply<<<nb, kScanThreads, 0, s.stream>>>(in, out, s.scan_part, n, nb);
+    launched(K_SCAN);
+}
+
+void run_enforce_pbc(State& s) {
+    if (s.N == 0) return;
+    GeoArgs a = geo_args(s.geo);
+    prof_begin(K_PBC);
+    k_enforce_pbc<<<nblocks(s.N, 256), 256, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.N, a);
+    launched(K_PBC);
+    prof_end(K_PBC);
+}
+
+void grow_atoms(State& s, int need);  // api.cu
+
+void run_borders(State& s) {
+    GeoArgs a = geo_args(s.geo);
+    const int N = s.N;
+    const int nblk = nblocks(N, 256);
+    if (N == 0) {
+        s.G = 0;
+        return;
+    }
+    prof_begin(K_BORDER);
+    k_border_count<<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.slot_of_ref, s.bmask, s.bcount, N, nblk, a);
+    launched(K_BORDER);
+    const int n = 26 * nblk;
+    // boff = exclusive scan of bcount, stored after the counts
+    int* boff = s.bcount + n;
+    exclusive_scan(s, s.bcount, boff, n);
+    TMD_CUDA(cudaMemcpyAsync(&s.status_host->nghost, boff + n, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    const int G = s.status_host->nghost;
+    if (N + G > s.capA) grow_atoms(s, N + G);
+    k_border_emit<<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
+                                              s.ref.b[s.ac], s.slot_of_ref, s.bmask, boff, s.gsrc, s.groot,
+                                              s.gcode, s.bsrc_ref, s.broot_ref, s.bcode, N, nblk, s.capA,
+                                              a, s.dem_fixed);
+    launched(K_BORDER);
+    prof_end(K_BORDER);
+    s.G = G;
+    s.lists_valid = 0;
+}
+
+void run_distribute(State& s) {
+    GeoArgs a = geo_args(s.geo);
+    const int N = s.N, NA = s.N + s.G;
+    const int nseg = 2 * (a.ncells + 1);
+    if (NA == 0) return;
+    prof_begin(K_BIN);
+    TMD_CUDA(cudaMemsetAsync(s.cnt, 0, sizeof(int) * nseg, s.stream));
+    TMD_CUDA(cudaMemsetAsync(&s.status_dev->out_local, 0, 2 * sizeof(int), s.stream));
+    k_bin_count<<<nblocks(NA, 256), 256, 0, s.stream>>>(s.pos.b[s.pc], s.cnt, s.bin_cell, s.bin_rank, s.status_dev,
+                                                        N, NA, a);
+    launched(K_BIN);
+    exclusive_scan(s, s.cnt, s.cstart, nseg);
+    k_bin_scatter<<<nblocks(NA, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.bin_cell, s.bin_rank, s.cstart,
+                                                          s.tmp_key, s.tmp_src, N, NA, a.ncells);
+    launched(K_BIN);
+    k_bin_rank<<<nblocks((long long)nseg * 32, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, s.perm,
+                                                                          nseg);
+    launched(K_BIN);
+    const int np = 1 - s.pc, nv = 1 - s.vc, na = 1 - s.ac;
+    k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
+        s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
+        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rbk, s.pos32, NA, N, a,
+        s.precision);
+    launched(K_BIN);
+    s.pc = np;
+    s.vc = nv;
+    s.ac = na;
+    if (s.G > 0) {
+        k_ghost_links<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.slot_of_ref, s.bsrc_ref, s.broot_ref,
+                                                               s.bcode, s.gsrc, s.groot, s.gcode, N, s.G);
+        launched(K_BIN);
+    }
+    prof_end(K_BIN);
+    s.lists_valid = 0;
+}
+
+void grow_lists(State& s, int rows);  // api.cu
+
+int run_build_lists(State& s, bool half, double cutoff) {
+    const Geometry& g = s.geo;
+    if (s.N == 0) {
+        s.lists_valid = 1;
+        s.lists_half = half;
+        return 0;
+    }
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        NlArgs a;
+        a.cut2 = cutoff * cutoff;
+        const double margin = 1e-3 * a.cut2 + 1e-6;
+        a.lo2 = (float)(a.cut2 - margin);
+        a.hi2 = (float)(a.cut2 + margin);
+        a.nbcap = s.nb_cap;
+        a.stride = s.nb_stride;
+        a.N = s.N;
+        a.ncells = g.ncells;
+        a.nx = g.nx;
+        a.nxy = g.nx * g.ny;
+        for (int d = 0; d < 3; ++d) a.alo[d] = g.aabb_lo[d];
+        a.spacing = g.spacing;
+        TMD_CUDA(cudaMemsetAsync(&s.status_dev->max_nb, 0, sizeof(int), s.stream));
+        TMD_CUDA(cudaMemsetAsync(&s.status_dev->bad_code, 0, sizeof(int), s.stream));
+        prof_begin(K_NLIST);
+        const int nb = nblocks(g.ncells, kNlWarps);
+        if (half)
+            k_build_list<true><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                   s.nbn, s.nbl, s.status_dev, a);
+        else
+            k_build_list<false><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                    s.nbn, s.nbl, s.status_dev, a);
+        launched(K_NLIST);
+        prof_end(K_NLIST);
+        TMD_CUDA(cudaMemcpyAsync(s.status_host, s.status_dev, sizeof(DevStatus), cudaMemcpyDeviceToHost, s.stream));
+        TMD_CUDA(cudaStreamSynchronize(s.stream));
+        if (s.status_host->out_local > 0) {
+            int first_out = 0;
+            // locals outside the grid sit at [cstart[ncells], N)
+            TMD_CUDA(cudaMemcpyAsync(&first_out, s.cstart + g.ncells, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+            TMD_CUDA(cudaStreamSynchronize(s.stream));
+            k_clear_lists<<<nblocks(s.N - first_out, 256), 256, 0, s.stream>>>(s.nbn, first_out, s.N);
+            launched(K_NLIST);
+            set_error(5, "locals outside the cell grid at binning (they have no neighbours)");
+        }
+        if (s.status_host->bad_code > 0 && s.precision == 1)
+            set_error(3, "list pair spans more than one rebasing cell; mixed forces are invalid");
+        const int mx = s.status_host->max_nb;
+        if (mx <= s.nb_cap) {
+            s.lists_valid = 1;
+            s.lists_half = half;
+            return 0;
+        }
+        // core/neighborlist.impala:74-76: grow to twice the overflow and redo
+        std::printf("0> reallocate_neighborlist_capacity(): %d\n", mx * 2);
+        grow_lists(s, mx * 2);
+    }
+    set_error(2, "neighbour list capacity did not converge");
+    return -1;
+}
+
+}  // namespace tmd

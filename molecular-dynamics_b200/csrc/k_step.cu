@@ -1,0 +1,694 @@
+// k_step.cu -- per-timestep kernels of the tinyMD B200 path:
+//   * LJ forces over full or half lists, FP64 (bit-identical to the CPU
+//     restatement for full lists) or mixed (FP32 pair arithmetic on rebased
+//     FP32 positions), optionally fused with the final velocity half-kick
+//     (core/compute.impala:79-126, core/runtime.impala:188-201, 186-194)
+//   * DEM spring-dashpot forces (core/runtime.impala:203-247)
+//   * initial integration fused with the periodic ghost refresh
+//     (core/compute.impala:175-184, comm/comm.impala:334-388)
+//   * stand-alone ghost refresh and final integration
+//   * deterministic FP64 reductions of energy, virial and kinetic energy
+//
+// Thread per local atom; the atom-fastest list makes the index loads of a
+// warp one coalesced 128-byte line per neighbour slot, and neighbour
+// positions come through the read-only path.
+
+#include "md_common.cuh"
+#include "md_state.h"
+
+namespace tmd {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kThermoQ = 4;  // partials: energy, virial, pairs inside the cutoff, v.v
+
+inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+struct StepArgs {
+    int N, G, stride;
+    double dt, h;  // h = 0.5 * dt as the reference computes it
+    double len[3], alo[3], rb_h;
+};
+
+struct LjArgs {
+    int N, stride, nbcap;
+    double rc2, sigma6, eps, h;
+    // mixed form
+    float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f;
+    float hx, hy, hz;  // -rb_h, -rb_h/4, -rb_h/16 (shift decode scales)
+};
+
+struct DemArgs {
+    int N, stride, nbcap, fixed;
+    double rc2, dn, dt_, k, mu, radius;
+};
+
+__device__ __forceinline__ double4 ldg_d4(const double4* p) {
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 a = __ldg(q), b = __ldg(q + 1);
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+// writes the per-block partial of quantity q (kThermoQ-major layout)
+__device__ __forceinline__ void put_partial(double* part, int q, double v, double* scratch) {
+    double r = block_sum(v, scratch);
+    if (threadIdx.x == 0) part[q * gridDim.x + blockIdx.x] = r;
+}
+
+// ---- FP64 LJ ------------------------------------------------------------------
+template <bool HALF, bool FUSE, bool THERMO>
+__global__ void __launch_bounds__(kThreads)
+k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* __restrict__ vel,
+          const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, double* __restrict__ part, LjArgs a) {
+    __shared__ double scratch[kThreads / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
+    if (i < a.N) {
+        const double4 pi = pos[i];
+        const int n = min(nbn[i], a.nbcap);
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        const uint32_t* lp = nbl + i;
+#pragma unroll 4
+        for (int k = 0; k < n; ++k) {
+            const int j = (int)(__ldg(lp + (size_t)k * a.stride) >> kCodeBits);
+            const double4 pj = ldg_d4(pos + j);
+            const double dx = dsub(pi.x, pj.x), dy = dsub(pi.y, pj.y), dz = dsub(pi.z, pj.z);
+            const double rsq = len2_strict(dx, dy, dz);
+            if (rsq < a.rc2) {
+                const double sr2 = ddiv(1.0, rsq);
+                const double sr6 = dmul(dmul(dmul(sr2, sr2), sr2), a.sigma6);
+                const double f = dmul(dmul(dmul(dmul(48.0, sr6), dsub(sr6, 0.5)), sr2), a.eps);
+                const double px = dmul(dx, f), py = dmul(dy, f), pz = dmul(dz, f);
+                fx = dadd(fx, px);
+                fy = dadd(fy, py);
+                fz = dadd(fz, pz);
+                if (HALF && j < a.N) {
+                    atomicAdd(&frc[j].x, -px);
+                    atomicAdd(&frc[j].y, -py);
+                    atomicAdd(&frc[j].z, -pz);
+                }
+                if (THERMO) {
+                    e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
+                    w += f * rsq;
+                    cnt += 1.0;
+                }
+            }
+        }
+        if (HALF) {
+            atomicAdd(&frc[i].x, fx);
+            atomicAdd(&frc[i].y, fy);
+            atomicAdd(&frc[i].z, fz);
+        } else {
+            frc[i] = make_double4(fx, fy, fz, 0.0);
+            if (FUSE) {  // core/compute.impala:186-194
+                double4 v = vel[i];
+                v.x = dadd(v.x, dmul(fx, a.h));
+                v.y = dadd(v.y, dmul(fy, a.h));
+                v.z = dadd(v.z, dmul(fz, a.h));
+                vel[i] = v;
+                if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
+            }
+        }
+    }
+    if (THERMO) {
+        put_partial(part, 0, e, scratch);
+        put_partial(part, 1, w, scratch);
+        put_partial(part, 2, cnt, scratch);
+        if (FUSE) put_partial(part, 3, ke, scratch);
+    }
+}
+
+// ---- mixed LJ -----------------------------------------------------------------
+// FP32 pair arithmetic on positions rebased to a dyadic grid of spacing rb_h:
+// del = (r_i - r_j) - dk*rb_h, with dk in {-1,0,1}^3 decoded from the list
+// entry's low bits and the product exact, so del carries one rounding more
+// than r_i - r_j.  Pairs closer than sigma (large forces, ~0.2 per atom in a
+// dense LJ liquid) and pairs within 1e-3 of the cutoff take the FP64 path, so
+// list membership and the cutoff test stay exactly the FP64 decisions.
+template <bool HALF, bool FUSE, bool THERMO>
+__global__ void __launch_bounds__(kThreads)
+k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
+           double4* __restrict__ vel, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
+           double* __restrict__ part, LjArgs a) {
+    __shared__ double scratch[kThreads / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
+    if (i < a.N) {
+        const float4 ri = pos32[i];
+        const int n = min(nbn[i], a.nbcap);
+        float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
+        double cx = 0.0, cy = 0.0, cz = 0.0;
+        int ncnt = 0;
+        const uint32_t* lp = nbl + i;
+#pragma unroll 4
+        for (int k = 0; k < n; ++k) {
+            const uint32_t ent = __ldg(lp + (size_t)k * a.stride);
+            const int j = (int)(ent >> kCodeBits);
+            const float4 rj = __ldg(pos32 + j);
+            const float sx = __int_as_float((int)((ent & 0x03u) | 0x4B000000u)) - 8388609.0f;
+            const float sy = __int_as_float((int)((ent & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
+            const float sz = __int_as_float((int)((ent & 0x30u) | 0x4B000000u)) - 8388624.0f;
+            const float dx = fmaf(a.hx, sx, ri.x - rj.x);
+            const float dy = fmaf(a.hy, sy, ri.y - rj.y);
+            const float dz = fmaf(a.hz, sz, ri.z - rj.z);
+            const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (rsq < a.rc2_hi) {
+                bool near = rsq >= a.rc2_lo || rsq < a.close2;
+                if (!near) {
+                    const float sr2 = __frcp_rn(rsq);
+                    const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
+                    const float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
+                    const float px = dx * f, py = dy * f, pz = dz * f;
+                    fx += px;
+                    fy += py;
+                    fz += pz;
+                    if (HALF && j < a.N) {
+                        atomicAdd(&frc32[j].x, -px);
+                        atomicAdd(&frc32[j].y, -py);
+                        atomicAdd(&frc32[j].z, -pz);
+                    }
+                    if (THERMO) {
+                        ef += a.eps4f * sr6 * (sr6 - 1.0f);
+                        wf += f * rsq;
+                        ncnt++;
+                    }
+                } else {
+                    // FP64 path: exact cutoff decision and close-contact accuracy
+                    const double4 pi = ldg_d4(pos + i);
+                    const double4 pj = ldg_d4(pos + j);
+                    const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
+                    const double r2 = len2_strict(ex, ey, ez);
+                    if (r2 < a.rc2) {
+                        const double sr2 = 1.0 / r2;
+                        const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
+                        const double f = 48.0 * sr6 * (sr6 - 0.5) * sr2 * a.eps;
+                        cx += ex * f;
+                        cy += ey * f;
+                        cz += ez * f;
+                        if (HALF && j < a.N) {
+                            atomicAdd(&frc32[j].x, (float)(-ex * f));
+                            atomicAdd(&frc32[j].y, (float)(-ey * f));
+                            atomicAdd(&frc32[j].z, (float)(-ez * f));
+                        }
+                        if (THERMO) {
+                            e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
+                            w += f * r2;
+                            ncnt++;
+                        }
+                    }
+                }
+            }
+        }
+        const double Fx = (double)fx + cx, Fy = (double)fy + cy, Fz = (double)fz + cz;
+        if (HALF) {
+            atomicAdd(&frc32[i].x, (float)Fx);
+            atomicAdd(&frc32[i].y, (float)Fy);
+            atomicAdd(&frc32[i].z, (float)Fz);
+        } else {
+            const float4 F = make_float4((float)Fx, (float)Fy, (float)Fz, 0.f);
+            frc32[i] = F;
+            if (FUSE) {
+                double4 v = vel[i];
+                v.x += (double)F.x * a.h;
+                v.y += (double)F.y * a.h;
+                v.z += (double)F.z * a.h;
+                vel[i] = v;
+                if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
+            }
+        }
+        if (THERMO) {
+            e += (double)ef;
+            w += (double)wf;
+            cnt = (double)ncnt;
+        }
+    }
+    if (THERMO) {
+        put_partial(part, 0, e, scratch);
+        put_partial(part, 1, w, scratch);
+        put_partial(part, 2, cnt, scratch);
+        if (FUSE) put_partial(part, 3, ke, scratch);
+    }
+}
+
+// ---- DEM ----------------------------------------------------------------------
+// core/runtime.impala:203-247.  With the reference condition the contact
+// branch can never run (penetration r - 2R > 0 inside r < 2R); `fixed`
+// selects the contact-fixed model (overlap 2R - r > 0, dissipative normal
+// spring-dashpot, Coulomb-capped tangential dashpot), which needs ghost
+// velocities (refreshed with the ghosts).
+__device__ __forceinline__ void dem_pair(const double4& del, double rsq, const double4& v1, const double4& v2,
+                                         const DemArgs& a, double* out) {
+    out[0] = out[1] = out[2] = 0.0;
+    const double radius = a.fixed ? a.radius : 1.0;
+    const double d2 = dmul(radius, 2.0);
+    if (!(rsq < dmul(d2, d2))) return;
+    const double len = __dsqrt_rn(rsq);
+    const double pen = dsub(len, d2);
+    if (!a.fixed) {
+        if (!(pen > 0.0)) return;
+        const double il = ddiv(1.0, len);
+        const double n[3] = {dmul(del.x, il), dmul(del.y, il), dmul(del.z, il)};
+        const double rv[3] = {dsub(v1.x, v2.x), dsub(v1.y, v2.y), dsub(v1.z, v2.z)};
+        const double vn = dadd(dadd(dmul(rv[0], n[0]), dmul(rv[1], n[1])), dmul(rv[2], n[2]));
+        const double vt[3] = {dsub(rv[0], dmul(n[0], vn)), dsub(rv[1], dmul(n[1], vn)), dsub(rv[2], dmul(n[2], vn))};
+        const double vtl = __dsqrt_rn(len2_strict(vt[0], vt[1], vt[2]));
+        const double fn = dsub(dmul(a.dn, vn), dmul(a.k, pen));
+        const double t1 = dmul(a.dt_, vtl), t2 = dmul(a.mu, fn);
+        const double ft = t1 < t2 ? t1 : t2;
+        const double iv = ddiv(1.0, vtl);
+        for (int d = 0; d < 3; ++d) out[d] = dadd(dmul(n[d], fn), dmul(dmul(vt[d], iv), ft));
+        return;
+    }
+    if (!(len > 0.0)) return;
+    const double delta = dsub(d2, len);
+    const double inv = ddiv(1.0, len);
+    const double n[3] = {dmul(del.x, inv), dmul(del.y, inv), dmul(del.z, inv)};
+    const double rv[3] = {dsub(v1.x, v2.x), dsub(v1.y, v2.y), dsub(v1.z, v2.z)};
+    const double vn = dadd(dadd(dmul(rv[0], n[0]), dmul(rv[1], n[1])), dmul(rv[2], n[2]));
+    const double vt[3] = {dsub(rv[0], dmul(n[0], vn)), dsub(rv[1], dmul(n[1], vn)), dsub(rv[2], dmul(n[2], vn))};
+    const double vtl = __dsqrt_rn(len2_strict(vt[0], vt[1], vt[2]));
+    double fn = dsub(dmul(a.k, delta), dmul(a.dn, vn));
+    if (fn < 0.0) fn = 0.0;
+    const double t1 = dmul(a.dt_, vtl), t2 = dmul(a.mu, fn);
+    const double ft = t1 < t2 ? t1 : t2;
+    const double tinv = vtl > 0.0 ? ddiv(1.0, vtl) : 0.0;
+    for (int d = 0; d < 3; ++d) out[d] = dsub(dmul(n[d], fn), dmul(dmul(vt[d], tinv), ft));
+}
+
+template <bool HALF>
+__global__ void __launch_bounds__(kThreads)
+k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, double4* __restrict__ frc,
+           const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, DemArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.N) return;
+    const double4 pi = pos[i];
+    const double4 vi = vel[i];
+    const int n = min(nbn[i], a.nbcap);
+    double F[3] = {0.0, 0.0, 0.0};
+    for (int k = 0; k < n; ++k) {
+        const int j = (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits);
+        const double4 pj = ldg_d4(pos + j);
+        const double4 del = make_double4(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z), 0.0);
+        const double rsq = len2_strict(del.x, del.y, del.z);
+        if (rsq < a.rc2) {
+            double f[3];
+            dem_pair(del, rsq, vi, ldg_d4(vel + j), a, f);
+            F[0] = dadd(F[0], f[0]);
+            F[1] = dadd(F[1], f[1]);
+            F[2] = dadd(F[2], f[2]);
+            if (HALF && j < a.N) {
+                atomicAdd(&frc[j].x, -f[0]);
+                atomicAdd(&frc[j].y, -f[1]);
+                atomicAdd(&frc[j].z, -f[2]);
+            }
+        }
+    }
+    if (HALF) {
+        atomicAdd(&frc[i].x, F[0]);
+        atomicAdd(&frc[i].y, F[1]);
+        atomicAdd(&frc[i].z, F[2]);
+    } else {
+        frc[i] = make_double4(F[0], F[1], F[2], 0.0);
+    }
+}
+
+// ---- integration + ghost refresh ------------------------------------------------
+// GM: 0 = locals only, ghost positions carried over unchanged;
+//     1 = reference two-phase refresh: ghost = (its source's value in this
+//         step) + one shift, where a local source is integrated here and a
+//         ghost source still holds the previous step's value (so chained
+//         edge / corner ghosts lag, exactly like comm/comm.impala:334-388);
+//     2 = exact periodic images: ghost = integrated root + total shift.
+__device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, double fx, double fy, double fz,
+                                                 double dt, double h) {
+    v.x = dadd(v.x, dmul(fx, h));
+    v.y = dadd(v.y, dmul(fy, h));
+    v.z = dadd(v.z, dmul(fz, h));
+    return make_double4(dadd(x.x, dmul(v.x, dt)), dadd(x.y, dmul(v.y, dt)), dadd(x.z, dmul(v.z, dt)), x.w);
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void load_force(const double4* frc, const float4* frc32, int i, double& fx, double& fy,
+                                           double& fz) {
+    if (MIXED) {
+        const float4 f = frc32[i];
+        fx = f.x; fy = f.y; fz = f.z;
+    } else {
+        const double4 f = frc[i];
+        fx = f.x; fy = f.y; fz = f.z;
+    }
+}
+
+template <int GM, bool MIXED, bool DEMV>
+__global__ void __launch_bounds__(kThreads)
+k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, const double4* __restrict__ vel_o,
+            double4* __restrict__ vel_n, const double4* __restrict__ frc, const float4* __restrict__ frc32,
+            float4* __restrict__ pos32, const int* __restrict__ rbk, const int* __restrict__ gsrc,
+            const int* __restrict__ groot, const int* __restrict__ gcode, StepArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < a.N) {
+        double4 v = vel_o[t];
+        double fx, fy, fz;
+        load_force<MIXED>(frc, frc32, t, fx, fy, fz);
+        const double4 x = integrate_one(pos_o[t], v, fx, fy, fz, a.dt, a.h);
+        pos_n[t] = x;
+        vel_n[t] = v;
+        if (MIXED) pos32[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
+        return;
+    }
+    if (t >= a.N + a.G) return;
+    const int g = t - a.N;
+    if (GM == 0) {
+        pos_n[t] = pos_o[t];
+        if (DEMV) vel_n[t] = vel_o[t];
+        return;
+    }
+    const int code = gcode[g];
+    const int s = GM == 1 ? gsrc[g] : groot[g];
+    double4 xs;
+    if (s < a.N) {
+        double4 vs = vel_o[s];
+        double fx, fy, fz;
+        load_force<MIXED>(frc, frc32, s, fx, fy, fz);
+        xs = integrate_one(pos_o[s], vs, fx, fy, fz, a.dt, a.h);
+    } else {
+        xs = pos_o[s];
+    }
+    const int base = GM == 1 ? 0 : 8;
+    double4 x;
+    x.x = dadd(xs.x, dmul(a.len[0], (double)shift_axis(code, base, 0)));
+    x.y = dadd(xs.y, dmul(a.len[1], (double)shift_axis(code, base, 1)));
+    x.z = dadd(xs.z, dmul(a.len[2], (double)shift_axis(code, base, 2)));
+    x.w = 0.0;
+    pos_n[t] = x;
+    if (MIXED) pos32[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
+    if (DEMV) {  // contact-fixed DEM: ghost velocity = its root's, after this half-kick
+        const int r = groot[g];
+        double4 vr = vel_o[r];
+        double fx, fy, fz;
+        load_force<MIXED>(frc, frc32, r, fx, fy, fz);
+        vr.x = dadd(vr.x, dmul(fx, a.h));
+        vr.y = dadd(vr.y, dmul(fy, a.h));
+        vr.z = dadd(vr.z, dmul(fz, a.h));
+        vel_n[t] = vr;
+    }
+}
+
+// stand-alone ghost refresh (no pending integration): locals carried over
+template <int GM, bool MIXED>
+__global__ void __launch_bounds__(kThreads)
+k_ghost_sync(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, float4* __restrict__ pos32,
+             double4* __restrict__ vel, int demv, const int* __restrict__ rbk, const int* __restrict__ gsrc,
+             const int* __restrict__ groot, const int* __restrict__ gcode, StepArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < a.N) {
+        pos_n[t] = pos_o[t];
+        return;
+    }
+    if (t >= a.N + a.G) return;
+    const int g = t - a.N;
+    const int code = gcode[g];
+    const int s = GM == 1 ? gsrc[g] : groot[g];
+    const double4 xs = pos_o[s];
+    const int base = GM == 1 ? 0 : 8;
+    double4 x;
+    x.x = dadd(xs.x, dmul(a.len[0], (double)shift_axis(code, base, 0)));
+    x.y = dadd(xs.y, dmul(a.len[1], (double)shift_axis(code, base, 1)));
+    x.z = dadd(xs.z, dmul(a.len[2], (double)shift_axis(code, base, 2)));
+    x.w = 0.0;
+    pos_n[t] = x;
+    if (MIXED) pos32[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
+    if (demv) vel[t] = vel[groot[g]];  // ghost slots only; roots are locals
+}
+
+template <bool MIXED, bool THERMO>
+__global__ void __launch_bounds__(kThreads)
+k_final(double4* __restrict__ vel, const double4* __restrict__ frc, const float4* __restrict__ frc32,
+        double* __restrict__ part, int N, double h) {
+    __shared__ double scratch[kThreads / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ke = 0.0;
+    if (i < N) {
+        double fx, fy, fz;
+        load_force<MIXED>(frc, frc32, i, fx, fy, fz);
+        double4 v = vel[i];
+        v.x = dadd(v.x, dmul(fx, h));
+        v.y = dadd(v.y, dmul(fy, h));
+        v.z = dadd(v.z, dmul(fz, h));
+        vel[i] = v;
+        if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
+    }
+    if (THERMO) put_partial(part, 3, ke, scratch);
+}
+
+__global__ void k_refresh_pos32(const double4* __restrict__ pos, float4* __restrict__ pos32,
+                                const int* __restrict__ rbk, int NA, StepArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < NA) pos32[t] = rebased32(pos[t], rbk[t], a.alo, a.rb_h);
+}
+
+__global__ void k_zero4(double4* __restrict__ d, float4* __restrict__ f, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    if (d) d[t] = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (f) f[t] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// sums part[q][0..nb) in a fixed order for q in [q0, q1) into out[q]
+__global__ void k_reduce_partials(const double* __restrict__ part, double* __restrict__ out, int nb, int q0,
+                                  int q1) {
+    __shared__ double scratch[32];
+    for (int q = q0; q < q1; ++q) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) v += part[q * nb + b];
+        double r = block_sum(v, scratch);
+        if (threadIdx.x == 0) out[q] = r;
+    }
+}
+
+StepArgs step_args(const State& s, double dt) {
+    StepArgs a;
+    a.N = s.N;
+    a.G = s.G;
+    a.stride = s.nb_stride;
+    a.dt = dt;
+    a.h = 0.5 * dt;
+    for (int d = 0; d < 3; ++d) {
+        a.len[d] = s.geo.len[d];
+        a.alo[d] = s.geo.aabb_lo[d];
+    }
+    a.rb_h = s.geo.rb_h;
+    return a;
+}
+
+double ipow(double x, int n) {  // utils/utilities.impala:27-36
+    if (n == 1) return x;
+    if (n % 2 == 0) {
+        double y = ipow(x, n / 2);
+        return y * y;
+    }
+    return x * ipow(x, n - 1);
+}
+
+template <bool HALF, bool FUSE, bool THERMO>
+void launch_lj(State& s, const LjArgs& a, int nb) {
+    double4* vel = s.vel.b[s.vc];
+    if (s.precision == 1)
+        k_lj_mixed<HALF, FUSE, THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos32, s.pos.b[s.pc], s.frc32, vel, s.nbn,
+                                                                     s.nbl, s.red_part, a);
+    else
+        k_lj_fp64<HALF, FUSE, THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn, s.nbl,
+                                                                    s.red_part, a);
+}
+
+}  // namespace
+
+void ensure_red_scratch(State& s, int n) {
+    if (n > s.red_part_cap) {
+        dfree(&s.red_part);
+        s.red_part_cap = n + 1024;
+        dalloc(&s.red_part, s.red_part_cap);
+    }
+}
+
+void run_reduce_thermo(State& s, int nb, int nq) {
+    (void)nq;
+    k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 0, kThermoQ);
+    launched(K_REDUCE);
+}
+
+void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
+    const int N = s.N;
+    if (N == 0) return;
+    LjArgs a;
+    a.N = N;
+    a.stride = s.nb_stride;
+    a.nbcap = s.nb_cap;
+    a.rc2 = p.rc * p.rc;
+    a.sigma6 = ipow(p.sigma, 6);
+    a.eps = p.eps;
+    a.h = 0.5 * dt;
+    const double margin = 1e-3 * a.rc2 + 1e-6;
+    a.rc2_lo = (float)(a.rc2 - margin);
+    a.rc2_hi = (float)(a.rc2 + margin);
+    a.close2 = (float)(p.sigma * p.sigma);
+    a.sig6f = (float)a.sigma6;
+    a.eps48f = (float)(48.0 * p.eps);
+    a.eps4f = (float)(4.0 * p.eps);
+    a.hx = (float)(-s.geo.rb_h);
+    a.hy = (float)(-s.geo.rb_h / 4.0);
+    a.hz = (float)(-s.geo.rb_h / 16.0);
+    const int nb = nblocks(N, kThreads);
+    const bool half = p.half;
+    const bool thermo = s.thermo != 0;
+    if (thermo) ensure_red_scratch(s, kThermoQ * nb);
+    if (half) {
+        if (s.precision == 1)
+            k_zero4<<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(nullptr, s.frc32, N);
+        else
+            k_zero4<<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.frc.b[s.ac], nullptr, N);
+        launched(K_MISC);
+        fuse_final = false;
+    }
+    prof_begin(K_FORCE_LJ);
+    if (half) {
+        if (thermo) launch_lj<true, false, true>(s, a, nb);
+        else launch_lj<true, false, false>(s, a, nb);
+    } else if (fuse_final) {
+        if (thermo) launch_lj<false, true, true>(s, a, nb);
+        else launch_lj<false, true, false>(s, a, nb);
+    } else {
+        if (thermo) launch_lj<false, false, true>(s, a, nb);
+        else launch_lj<false, false, false>(s, a, nb);
+    }
+    launched(K_FORCE_LJ);
+    prof_end(K_FORCE_LJ);
+    if (fuse_final) s.integration_iters = N;
+    if (thermo) {
+        if (!fuse_final) {
+            // energy/virial only; the kinetic partial comes from the next final kick
+            k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 0, 3);
+        } else {
+            k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 0, kThermoQ);
+        }
+        launched(K_REDUCE);
+    }
+}
+
+void run_force_dem(State& s, const PendingForce& p) {
+    const int N = s.N;
+    if (N == 0) return;
+    DemArgs a;
+    a.N = N;
+    a.stride = s.nb_stride;
+    a.nbcap = s.nb_cap;
+    a.fixed = s.dem_fixed;
+    a.rc2 = p.rc * p.rc;
+    a.dn = p.dn;
+    a.dt_ = p.dt_;
+    a.k = p.k;
+    a.mu = p.mu;
+    a.radius = s.dem_radius;
+    if (p.half) {
+        k_zero4<<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.frc.b[s.ac], nullptr, N);
+        launched(K_MISC);
+    }
+    prof_begin(K_FORCE_DEM);
+    if (p.half)
+        k_dem_fp64<true><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc],
+                                                                          s.frc.b[s.ac], s.nbn, s.nbl, a);
+    else
+        k_dem_fp64<false><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc],
+                                                                           s.frc.b[s.ac], s.nbn, s.nbl, a);
+    launched(K_FORCE_DEM);
+    prof_end(K_FORCE_DEM);
+}
+
+void run_integrate(State& s, double dt, bool fuse_ghosts) {
+    const int NA = s.N + s.G;
+    if (NA == 0) return;
+    StepArgs a = step_args(s, dt);
+    const int gm = fuse_ghosts ? (s.ghost_exact ? 2 : 1) : 0;
+    const bool mixed = s.precision == 1;
+    const bool demv = s.dem_fixed != 0;
+    const double4* po = s.pos.b[s.pc];
+    double4* pn = s.pos.b[1 - s.pc];
+    const double4* vo = s.vel.b[s.vc];
+    double4* vn = s.vel.b[1 - s.vc];
+    const int nb = nblocks(NA, kThreads);
+#define TMD_INT(GM_, MX_, DV_)                                                                                 \
+    k_integrate<GM_, MX_, DV_><<<nb, kThreads, 0, s.stream>>>(po, pn, vo, vn, s.frc.b[s.ac], s.frc32, s.pos32, \
+                                                              s.rbk, s.gsrc, s.groot, s.gcode, a)
+    prof_begin(K_INTEGRATE);
+    if (gm == 0) {
+        if (mixed) { if (demv) TMD_INT(0, true, true); else TMD_INT(0, true, false); }
+        else { if (demv) TMD_INT(0, false, true); else TMD_INT(0, false, false); }
+    } else if (gm == 1) {
+        if (mixed) { if (demv) TMD_INT(1, true, true); else TMD_INT(1, true, false); }
+        else { if (demv) TMD_INT(1, false, true); else TMD_INT(1, false, false); }
+    } else {
+        if (mixed) { if (demv) TMD_INT(2, true, true); else TMD_INT(2, true, false); }
+        else { if (demv) TMD_INT(2, false, true); else TMD_INT(2, false, false); }
+    }
+#undef TMD_INT
+    launched(K_INTEGRATE);
+    prof_end(K_INTEGRATE);
+    s.pc = 1 - s.pc;
+    s.vc = 1 - s.vc;
+    s.integration_iters = s.N;
+}
+
+void run_ghost_sync(State& s) {
+    const int NA = s.N + s.G;
+    if (NA == 0) return;
+    StepArgs a = step_args(s, 0.0);
+    const double4* po = s.pos.b[s.pc];
+    double4* pn = s.pos.b[1 - s.pc];
+    const int nb = nblocks(NA, kThreads);
+    prof_begin(K_GHOST_SYNC);
+    if (s.ghost_exact) {
+        if (s.precision == 1) k_ghost_sync<2, true><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+        else k_ghost_sync<2, false><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+    } else {
+        if (s.precision == 1) k_ghost_sync<1, true><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+        else k_ghost_sync<1, false><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+    }
+    launched(K_GHOST_SYNC);
+    prof_end(K_GHOST_SYNC);
+    s.pc = 1 - s.pc;
+}
+
+void run_final(State& s, double dt) {
+    const int N = s.N;
+    if (N == 0) return;
+    const int nb = nblocks(N, kThreads);
+    const bool thermo = s.thermo != 0;
+    if (thermo) ensure_red_scratch(s, kThermoQ * nb);
+    prof_begin(K_FINAL);
+    const double h = 0.5 * dt;
+    if (s.precision == 1) {
+        if (thermo) k_final<true, true><<<nb, kThreads, 0, s.stream>>>(s.vel.b[s.vc], s.frc.b[s.ac], s.frc32, s.red_part, N, h);
+        else k_final<true, false><<<nb, kThreads, 0, s.stream>>>(s.vel.b[s.vc], s.frc.b[s.ac], s.frc32, s.red_part, N, h);
+    } else {
+        if (thermo) k_final<false, true><<<nb, kThreads, 0, s.stream>>>(s.vel.b[s.vc], s.frc.b[s.ac], s.frc32, s.red_part, N, h);
+        else k_final<false, false><<<nb, kThreads, 0, s.stream>>>(s.vel.b[s.vc], s.frc.b[s.ac], s.frc32, s.red_part, N, h);
+    }
+    launched(K_FINAL);
+    prof_end(K_FINAL);
+    if (thermo) {
+        k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 3, 4);
+        launched(K_REDUCE);
+    }
+    s.integration_iters = N;
+}
+
+void run_refresh_pos32(State& s) {
+    const int NA = s.N + s.G;
+    if (NA == 0) return;
+    StepArgs a = step_args(s, 0.0);
+    k_refresh_pos32<<<nblocks(NA, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.pos32, s.rbk, NA, a);
+    launched(K_MISC);
+}
+
+}  // namespace tmd

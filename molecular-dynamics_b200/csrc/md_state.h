@@ -1,0 +1,189 @@
+// md_state.h -- host-side state of the tinyMD B200 library and the launch
+// wrappers of its kernels.  One global State instance (the reference keeps
+// one global grid too, core/runtime.impala:1-2).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+namespace tmd {
+
+enum Phase { PH_FORCE = 1, PH_NEIGH = 2, PH_COMM = 3, PH_BALANCE = 4, PH_OTHER = 5, PH_COUNT = 6 };
+
+enum KernelId {
+    K_FORCE_LJ = 0,   // LJ forces (any list / precision), possibly fused with the final kick
+    K_FORCE_DEM,
+    K_INTEGRATE,      // initial integration (+ ghost refresh when fused)
+    K_GHOST_SYNC,     // stand-alone ghost refresh
+    K_FINAL,          // stand-alone final integration
+    K_PBC,
+    K_BORDER,         // ghost generation (3 kernels)
+    K_BIN,            // counting sort (5 kernels)
+    K_NLIST,          // neighbour-list build
+    K_SCAN,
+    K_REDUCE,
+    K_HVP,            // adjoint Hessian-vector product
+    K_ADJ_STEP,       // adjoint elementwise updates
+    K_MISC,
+    K_COUNT
+};
+const char* kernel_name(int id);
+
+template <class T>
+struct DBuf {  // a double-buffered device array
+    T* b[2] = {nullptr, nullptr};
+};
+
+struct Geometry {
+    double world_lo[3], world_hi[3];
+    double aabb_lo[3], aabb_hi[3];  // rank box extended by one cell spacing
+    double len[3];                  // world lengths (periodic shifts)
+    double spacing;
+    int nx, ny, nz, ncells;
+    // mixed form: dyadic rebasing grid (spacing rb_h > list cutoff)
+    double rb_h;
+};
+
+// Device-side status words written by kernels and read back with one copy.
+struct DevStatus {
+    int nghost;         // ghosts produced by the last border pass
+    int max_nb;         // longest neighbour list of the last build
+    int out_local;      // locals outside the cell grid at the last binning
+    int out_ghost;      // ghosts outside the cell grid
+    int bad_code;       // list pairs whose rebasing offset exceeded one cell
+    int pad[3];
+};
+
+struct PendingForce {
+    bool valid = false;
+    bool dem = false;
+    bool half = false;
+    double rc = 0, eps = 0, sigma = 0;
+    double dn = 0, dt_ = 0, k = 0, mu = 0;
+};
+
+struct State {
+    bool alive = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Geometry geo{};
+
+    // sizes
+    int N = 0, G = 0;
+    int capA = 0;       // slots for locals + ghosts
+    int nb_cap = 0;     // neighbour-list capacity per atom (rows)
+    int nb_stride = 0;  // column stride of the atom-fastest list
+    int nblk_border = 0;
+    int lists_valid = 0;
+    bool lists_half = false;
+
+    // modes
+    int precision = 0;   // 0 FP64, 1 mixed
+    int ghost_exact = 0;
+    int dem_fixed = 0;
+    double dem_radius = 1.0;
+    int thermo = 0;
+
+    // device arrays (slots: locals 0..N-1 sorted by cell, ghosts N..N+G-1)
+    DBuf<double4> pos;   int pc = 0;   // positions
+    DBuf<double4> vel;   int vc = 0;   // velocities
+    DBuf<double4> frc;   DBuf<double> mass;  DBuf<int> ref;  DBuf<int> img;  int ac = 0;
+    float4* frc32 = nullptr;   // mixed-form forces
+    float4* pos32 = nullptr;   // mixed-form rebased positions
+    int* rbk = nullptr;        // packed rebasing cell of each slot
+    int* slot_of_ref = nullptr;
+    int* gsrc = nullptr;       // ghost: source slot (reference two-phase refresh)
+    int* groot = nullptr;      // ghost: root local slot
+    int* gcode = nullptr;      // ghost: shifts (see md_common.cuh)
+    // cells: starts of locals per cell [ncells+2] followed by ghosts per cell [ncells+2]
+    int* cnt = nullptr;        // counts, same layout
+    int* cstart = nullptr;     // exclusive scan of cnt (ghost starts include the N offset)
+    int* bin_cell = nullptr;   // per slot: cell of the slot (or ncells when outside)
+    int* bin_rank = nullptr;   // per slot: arrival rank within its cell
+    int* tmp_key = nullptr;    // per sorted position: reference index
+    int* tmp_src = nullptr;    // per sorted position: old slot
+    int* perm = nullptr;       // new slot -> old slot
+    // border pass
+    unsigned* bmask = nullptr;   // per local (reference order): 26-bit ghost-type mask
+    int* bcount = nullptr;       // [26][nblk] counts, scanned in place
+    int* bsrc_ref = nullptr;     // per ghost (reference order): source reference index
+    int* broot_ref = nullptr;    // per ghost: root local reference index
+    int* bcode = nullptr;        // per ghost: shift code (reference order)
+    // neighbour lists
+    int* nbn = nullptr;
+    uint32_t* nbl = nullptr;
+    // scan scratch, reductions, status
+    int* scan_part = nullptr;  int scan_part_cap = 0;
+    double* red_part = nullptr; int red_part_cap = 0;
+    double* thermo_dev = nullptr;   // [8]
+    DevStatus* status_dev = nullptr;
+    DevStatus* status_host = nullptr;  // pinned
+    double* thermo_host = nullptr;     // pinned [8]
+
+    // host mirror in reference order (core/grid.impala ArrayData host buffers)
+    std::vector<double> h_mass;                 // [N+G]
+    std::vector<double> h_pos, h_vel, h_frc;    // [(N+G)*3]
+    std::vector<double> h_x0;                   // initial positions (adjoint)
+
+    PendingForce pend_force;
+    bool pend_init = false;
+    double pend_dt = 0.0;
+
+    // reported iteration counters (core/runtime.impala:3-5)
+    long long force_iters = 0, rsq_iters = 0, integration_iters = 0;
+    int last_force_half = 0;
+    double last_rc = 0, last_eps = 0, last_sigma = 0;
+
+    // bookkeeping
+    long long launches = 0;
+    long long dev_bytes = 0;
+    int last_error = 0;
+    std::string last_error_msg;
+};
+
+extern State g_state;
+
+// ---- error helpers ---------------------------------------------------------
+void set_error(int code, const std::string& msg);
+bool cuda_ok(cudaError_t e, const char* what);
+#define TMD_CUDA(call) ::tmd::cuda_ok((call), #call)
+void launched(int kernel_id);  // counts a launch, checks the launch error
+
+// ---- timing ------------------------------------------------------------------
+void phase_mark(int phase);
+void phase_times(double* out6);
+void phase_reset();
+void prof_begin(int kernel_id);
+void prof_end(int kernel_id);
+void prof_reset();
+
+// ---- kernels (launch wrappers, all on g_state.stream) ---------------------
+struct KLaunch;  // fwd
+void run_enforce_pbc(State& s);
+void run_borders(State& s);                       // ghost generation, reference order
+void run_distribute(State& s);                    // binning + reorder
+int run_build_lists(State& s, bool half, double cutoff);  // returns 0 or error
+void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt);
+void run_force_dem(State& s, const PendingForce& p);
+void run_integrate(State& s, double dt, bool fuse_ghosts);
+void run_ghost_sync(State& s);
+void run_final(State& s, double dt);
+void run_refresh_pos32(State& s);
+void run_reduce_thermo(State& s, int nblocks, int nq);
+void exclusive_scan(State& s, const int* in, int* out, int n);
+void ensure_scan_scratch(State& s, int n);
+void ensure_red_scratch(State& s, int n);
+
+// device memory helpers
+void dev_alloc(void** p, size_t bytes);
+void dev_free(void** p);
+template <class T>
+inline void dalloc(T** p, size_t n) { dev_alloc(reinterpret_cast<void**>(p), n * sizeof(T)); }
+template <class T>
+inline void dfree(T** p) { dev_free(reinterpret_cast<void**>(p)); }
+
+}  // namespace tmd

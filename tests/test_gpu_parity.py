@@ -1,0 +1,131 @@
+"""Parity of the CUDA path against the CPU oracle, through the md_* C ABI.
+
+Both libraries run the same calls on the same seeded lattice.  The FP64 form
+with full lists is expected to be bit-identical to the oracle (same list
+order, same operand order, no FMA contraction); half lists sum in a
+different order (atomics) and are compared at 1e-12 relative.
+"""
+import numpy as np
+import pytest
+
+import tinymd
+from helpers import lists_as_sets, make_sim, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def both(product, oracle, **kw):
+    a = make_sim(product, setup_lib=product, **kw)
+    b = make_sim(oracle, setup_lib=product, **kw)
+    return a, b
+
+
+def close_all(*sims):
+    for s in sims:
+        s.close()
+
+
+def assert_same_ghosts(product, oracle):
+    gp, go = tinymd.ghost_info(product), tinymd.ghost_info(oracle)
+    assert product.md_get_number_of_ghost_particles() == oracle.md_get_number_of_ghost_particles()
+    for a, b, name in zip(gp, go, ("src", "pbc", "root", "tshift")):
+        np.testing.assert_array_equal(a, b, err_msg=name)
+
+
+@pytest.mark.parametrize("cells", [(8, 8, 8), (5, 7, 6)])
+def test_initial_ghosts_lists_forces_bitwise(product, oracle, cells):
+    p, o = both(product, oracle, cells=cells)
+    try:
+        assert p.counts() == o.counts()
+        assert_same_ghosts(product, oracle)
+        lp = tinymd.neighbor_lists(product, p.n)
+        lo = tinymd.neighbor_lists(oracle, o.n)
+        for i, (a, b) in enumerate(zip(lp, lo)):
+            np.testing.assert_array_equal(a, b, err_msg=f"list of atom {i}")
+        xp, vp, fp = tinymd.full_state(product)
+        xo, vo, fo = tinymd.full_state(oracle)
+        np.testing.assert_array_equal(xp, xo)
+        np.testing.assert_array_equal(vp, vo)
+        np.testing.assert_array_equal(fp, fo)
+    finally:
+        close_all(p, o)
+
+
+def test_trajectory_bitwise_fp64_full(product, oracle):
+    """100 steps (5 reneighbourings, lagged ghosts): positions, velocities, forces bit-identical."""
+    p, o = both(product, oracle, cells=(8, 8, 8))
+    try:
+        for chunk in range(10):
+            p.step(0.005, 10)
+            o.step(0.005, 10)
+            xp, vp, fp = tinymd.full_state(product)
+            xo, vo, fo = tinymd.full_state(oracle)
+            assert xp.shape == xo.shape
+            np.testing.assert_array_equal(xp, xo, err_msg=f"positions after {10 * (chunk + 1)} steps")
+            np.testing.assert_array_equal(vp, vo)
+            np.testing.assert_array_equal(fp, fo)
+        assert_same_ghosts(product, oracle)
+        # the host-mirror path of the reference interface agrees too
+        mp, xp2, vp2, fp2 = p.arrays()
+        mo, xo2, vo2, fo2 = o.arrays()
+        np.testing.assert_array_equal(xp2, xo2)
+        np.testing.assert_array_equal(vp2, vo2)
+        gp, go = p.ghost_arrays(), o.ghost_arrays()
+        np.testing.assert_array_equal(gp[1], go[1])
+    finally:
+        close_all(p, o)
+
+
+def test_trajectory_exact_ghosts(product, oracle):
+    product.md_set_ghost_mode(1)
+    oracle.oracle_set_ghost_mode(1)
+    p, o = both(product, oracle, cells=(6, 6, 6))
+    try:
+        p.step(0.005, 45)
+        o.step(0.005, 45)
+        xp, vp, fp = tinymd.full_state(product)
+        xo, vo, fo = tinymd.full_state(oracle)
+        np.testing.assert_array_equal(xp, xo)
+        np.testing.assert_array_equal(vp, vo)
+    finally:
+        close_all(p, o)
+        product.md_set_ghost_mode(0)
+        oracle.oracle_set_ghost_mode(0)
+
+
+def test_half_lists(product, oracle):
+    p, o = both(product, oracle, cells=(8, 8, 8), half=True)
+    try:
+        lp = tinymd.neighbor_lists(product, p.n)
+        lo = tinymd.neighbor_lists(oracle, o.n)
+        for a, b in zip(lp, lo):
+            np.testing.assert_array_equal(a, b)
+            assert np.all(a < p.n)  # the reference's half lists hold no ghosts
+        _, _, fp = tinymd.full_state(product)
+        _, _, fo = tinymd.full_state(oracle)
+        assert rel_err(fp, fo) < 1e-12
+        p.step(0.005, 10)
+        o.step(0.005, 10)
+        xp, vp, fp = tinymd.full_state(product)
+        xo, vo, fo = tinymd.full_state(oracle)
+        assert rel_err(xp, xo) < 1e-10
+        assert rel_err(fp, fo) < 1e-10
+    finally:
+        close_all(p, o)
+
+
+def test_mixed_force_error(product, oracle):
+    """Mixed form on the FP64 form's own positions: max |dF| / rms(F) <= 1e-5."""
+    p = make_sim(product, setup_lib=product, cells=(8, 8, 8))
+    try:
+        p.step(0.005, 60)
+        _, _, f64 = tinymd.full_state(product)
+        product.md_set_precision(1)
+        p.force()
+        product.md_final_integration(0.0)
+        _, _, f32 = tinymd.full_state(product)
+        err = rel_err(f32, f64)
+        assert err <= 1e-5, err
+    finally:
+        product.md_set_precision(0)
+        p.close()
