@@ -153,6 +153,12 @@ void md_set_precision(int mode);
  * lag by one step per chain link, comm/comm.impala:334-388; default),
  * 1 = exact periodic images (ghost = root local + total shift). */
 void md_set_ghost_mode(int exact);
+/* Half neighbour lists: 0 = the reference's (core/neighborlist.impala:34 keeps
+ * j < i by particle index, which never admits a ghost, so every pair across
+ * the periodic boundary is dropped; default), 1 = corrected: local-ghost
+ * pairs are kept when the ghost's root local precedes i, and the reaction
+ * force goes to that root. */
+void md_set_half_mode(int ghost_pairs);
 /* DEM contact model: 0 = the reference closure (its contact branch is
  * unreachable, so the force is zero; default), 1 = contact-fixed
  * spring-dashpot with contact radius `radius` (overlap 2R - r > 0). */
@@ -183,6 +189,17 @@ void md_profile_reset(void);
 long long md_kernel_launches(void);
 /* Device bytes held by the library. */
 long long md_device_bytes(void);
+
+/* Runs `steps` timesteps of the md driver loop (main.cpp:715-776) natively:
+ * initial integration, ghost refresh -- or, when (step0 + k + 1) is a
+ * multiple of reneigh_every, exchange / wrap / borders / binning / lists with
+ * `list_cutoff` -- then the force of the last md_compute_* call and the final
+ * integration.  When step_ms is not NULL each step is bracketed by CUDA
+ * events and its device time stored; when flush_buf is not NULL, flush_bytes
+ * of it are overwritten before each step, outside the timed interval (an L2
+ * flush for benchmarking).  Returns 0 on success. */
+int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double list_cutoff, float *step_ms,
+                     void *flush_buf, long long flush_bytes);
 
 /* Parity introspection (reference index space: locals 0..N-1 in input order,
  * ghosts N..N+G-1 in the reference's ghost order).  Drain pending work. */

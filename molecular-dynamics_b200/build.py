@@ -24,8 +24,7 @@ OBJ = os.path.join(LIB, "obj")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-v" if os.environ.get("TMD_PTXAS_V") else "-O3",
-                  "-I" + INC, "-I" + CSRC, "-I" + HOST]
+NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC, "-I" + HOST]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + INC, "-I" + HOST]
 
 CU_SOURCES = ["api.cu", "k_neigh.cu", "k_step.cu", "adjoint.cu"]

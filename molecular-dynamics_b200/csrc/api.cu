@@ -211,7 +211,7 @@ void free_all(State& s) {
         dfree(&s.ref.b[b]);
         dfree(&s.img.b[b]);
     }
-    int** ip[] = {&s.rbk, &s.slot_of_ref, &s.gsrc, &s.groot, &s.gcode, &s.cnt, &s.cstart, &s.bin_cell,
+    int** ip[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.cnt, &s.cstart, &s.bin_cell,
                   &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.bcount, &s.bsrc_ref, &s.broot_ref, &s.bcode,
                   &s.nbn, &s.scan_part};
     for (int** q : ip) dfree(q);
@@ -244,7 +244,8 @@ void grow_atoms(State& s, int need) {
     }
     realloc_keep(&s.frc32, o, n, s.stream);
     realloc_keep(&s.pos32, o, n, s.stream);
-    int** keep[] = {&s.rbk, &s.slot_of_ref, &s.gsrc, &s.groot, &s.gcode, &s.bsrc_ref, &s.broot_ref, &s.bcode};
+    int** keep[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.bsrc_ref, &s.broot_ref,
+                    &s.bcode};
     for (int** q : keep) realloc_keep(q, o, n, s.stream);
     int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.nbn};
     for (int** q : scratch) {
@@ -424,6 +425,7 @@ void md_set_stream(void* stream) {
     }
     s.stream = (cudaStream_t)stream;
     s.own_stream = false;
+    s.stream_set = true;
 }
 
 // core/runtime.impala:7-37
@@ -444,7 +446,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     }
     if (s.alive) md_deallocate_grid();
     TMD_CUDA(cudaGetDevice(&s.device));
-    if (!s.stream) {
+    if (!s.stream && !s.stream_set) {
         TMD_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
         s.own_stream = true;
     }
@@ -647,6 +649,7 @@ void md_compute_lennard_jones(bool half, double rc, double eps, double sigma) {
     p.eps = eps;
     p.sigma = sigma;
     s.pend_force = p;
+    s.force_cfg = p;
     s.last_rc = rc;
     s.last_eps = eps;
     s.last_sigma = sigma;
@@ -666,6 +669,7 @@ void md_compute_dem(bool half, double rc, double damping_n, double damping_t, do
     p.k = stiffness;
     p.mu = friction;
     s.pend_force = p;
+    s.force_cfg = p;
 }
 
 void md_final_integration(double dt) {
@@ -907,6 +911,11 @@ void md_set_precision(int mode) {
     }
     s.precision = mode;
 }
+void md_set_half_mode(int ghost_pairs) {
+    if (g_state.alive) flush_all(g_state);
+    g_state.half_ghost = ghost_pairs ? 1 : 0;
+    g_state.lists_valid = 0;
+}
 void md_set_ghost_mode(int exact) {
     if (g_state.alive) flush_all(g_state);
     g_state.ghost_exact = exact ? 1 : 0;
@@ -1070,6 +1079,51 @@ int md_get_cell_sizes(int* out, int ncells) {
     sync_stream(s);
     for (int k = 0; k < nc && k < ncells; ++k) out[k] = c[k] + c[nc + 1 + k];
     return nc;
+}
+
+// The md driver's timestep loop (main.cpp:715-776) issued natively.
+int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double list_cutoff, float* step_ms,
+                     void* flush_buf, long long flush_bytes) {
+    State& s = g_state;
+    if (!require_alive("md_run_timesteps")) return -1;
+    if (!s.force_cfg.valid || reneigh_every <= 0 || steps < 0) {
+        set_error(MD_ERR_STATE, "md_run_timesteps: no force configured (call md_compute_* once) or bad arguments");
+        return -1;
+    }
+    flush_all(s);
+    std::vector<cudaEvent_t> ev;
+    if (step_ms) {
+        ev.resize(2 * (size_t)steps);
+        for (auto& e : ev) TMD_CUDA(cudaEventCreate(&e));
+    }
+    const PendingForce cfg = s.force_cfg;
+    for (int k = 0; k < steps; ++k) {
+        if (flush_buf && flush_bytes > 0)
+            TMD_CUDA(cudaMemsetAsync(flush_buf, (k & 0x7f) + 1, (size_t)flush_bytes, s.stream));
+        if (step_ms) TMD_CUDA(cudaEventRecord(ev[2 * k], s.stream));
+        md_initial_integration(dt);
+        if ((step0 + k + 1) % reneigh_every == 0) {
+            md_exchange_particles();
+            md_enforce_pbc();
+            md_borders();
+            md_distribute_particles();
+            md_assemble_neighborlists(cfg.half, list_cutoff);
+        } else {
+            md_synchronize_ghost_layer();
+        }
+        if (cfg.dem) md_compute_dem(cfg.half, cfg.rc, cfg.dn, cfg.dt_, cfg.k, cfg.mu);
+        else md_compute_lennard_jones(cfg.half, cfg.rc, cfg.eps, cfg.sigma);
+        md_final_integration(dt);
+        if (step_ms) TMD_CUDA(cudaEventRecord(ev[2 * k + 1], s.stream));
+    }
+    sync_stream(s);
+    for (int k = 0; step_ms && k < steps; ++k) {
+        float ms = 0.f;
+        TMD_CUDA(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
+        step_ms[k] = ms;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    return s.last_error == MD_ERR_CUDA ? -1 : 0;
 }
 
 int md_get_grid_info(int* out) {

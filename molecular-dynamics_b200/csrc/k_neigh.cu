@@ -262,12 +262,18 @@ __global__ void k_bin_scatter(const int* __restrict__ ref, const int* __restrict
 }
 
 // One warp per segment: rank members by reference index (keys are unique).
+// The two outside-the-grid buckets keep arrival order: their members have no
+// neighbours and are nobody's neighbour, so their order is not observable.
 __global__ void k_bin_rank(const int* __restrict__ cstart, const int* __restrict__ tmp_key,
-                           const int* __restrict__ tmp_src, int* __restrict__ perm, int nseg) {
+                           const int* __restrict__ tmp_src, int* __restrict__ perm, int nseg, int ncells) {
     int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
     if (w >= nseg) return;
     int a = cstart[w], b = cstart[w + 1];
+    if (w == ncells || w == 2 * ncells + 1) {
+        for (int e = a + lane; e < b; e += 32) perm[e] = tmp_src[e];
+        return;
+    }
     for (int e = a + lane; e < b; e += 32) {
         int key = tmp_key[e];
         int rank = 0;
@@ -281,7 +287,8 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
                           const double4* __restrict__ frc_o, double4* __restrict__ frc_n,
                           const double* __restrict__ mass_o, double* __restrict__ mass_n,
                           const int* __restrict__ ref_o, int* __restrict__ ref_n, const int* __restrict__ img_o,
-                          int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rbk,
+                          int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rref,
+                          int* __restrict__ rbk,
                           float4* __restrict__ pos32, int NA, int N, GeoArgs a, int mixed) {
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= NA) return;
@@ -293,7 +300,10 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
     mass_n[n] = mass_o[o];
     int r = ref_o[o];
     ref_n[n] = r;
-    if (n < N) img_n[n] = img_o[o];
+    if (n < N) {
+        img_n[n] = img_o[o];
+        rref[n] = r;
+    }
     slot_of_ref[r] = n;
     int k = rebase_cell(p, a);
     rbk[n] = k;
@@ -303,13 +313,14 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
 __global__ void k_ghost_links(const int* __restrict__ ref, const int* __restrict__ slot_of_ref,
                               const int* __restrict__ bsrc_ref, const int* __restrict__ broot_ref,
                               const int* __restrict__ bcode, int* __restrict__ gsrc, int* __restrict__ groot,
-                              int* __restrict__ gcode, int N, int G) {
+                              int* __restrict__ gcode, int* __restrict__ rref, int N, int G) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= G) return;
     int g = ref[N + h] - N;
     gsrc[h] = slot_of_ref[bsrc_ref[g]];
     groot[h] = slot_of_ref[broot_ref[g]];
     gcode[h] = bcode[g];
+    rref[N + h] = broot_ref[g];
 }
 
 // ---- neighbour lists ---------------------------------------------------------
@@ -324,7 +335,7 @@ struct NlArgs {
     double alo[3], spacing;
 };
 
-template <bool HALF>
+template <int HM>
 __global__ void __launch_bounds__(kNlWarps * 32)
 k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
              const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl,
@@ -398,7 +409,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                     double4 p = pos[slot];
                     s_cpos[wid][m - t0] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]),
                                                       (float)(p.z - ctr[2]), __int_as_float(slot));
-                    s_cref[wid][m - t0] = HALF ? ref[slot] : 0;
+                    s_cref[wid][m - t0] = HM ? ref[slot] : 0;  // root reference index (ref for locals)
                     s_crbk[wid][m - t0] = rbk[slot];
                 }
             }
@@ -406,7 +417,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
             for (int h = 0; h < hn; ++h) {
                 const int i = hb + h;
                 const float4 hp = s_hpos[wid][h];
-                const int iref = HALF ? ref[i] : 0;
+                const int iref = HM ? ref[i] : 0;
                 const int irbk = rbk[i];
                 int cnt = s_hcnt[wid][h];
                 for (int q0 = 0; q0 < tn; q0 += 32) {
@@ -425,7 +436,10 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                             const double4 pi = pos[i], pj = pos[slot];
                             in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
                         }
-                        pred = in && slot != i && (!HALF || s_cref[wid][q] < iref);
+                        // core/neighborlist.impala:34: half lists keep i > j (reference index);
+                        // HM == 2 compares ghosts by their root so pairs across the
+                        // periodic boundary are kept once
+                        pred = in && slot != i && (!HM || s_cref[wid][q] < iref);
                         if (pred) {
                             const int cr = s_crbk[wid][q];
                             int dkx = wrap_diff(unpack_axis(cr, 0), unpack_axis(irbk, 0));
@@ -624,12 +638,12 @@ void run_distribute(State& s) {
                                                           s.tmp_key, s.tmp_src, N, NA, a.ncells);
     launched(K_BIN);
     k_bin_rank<<<nblocks((long long)nseg * 32, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, s.perm,
-                                                                          nseg);
+                                                                          nseg, a.ncells);
     launched(K_BIN);
     const int np = 1 - s.pc, nv = 1 - s.vc, na = 1 - s.ac;
     k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
         s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
-        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rbk, s.pos32, NA, N, a,
+        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk, s.pos32, NA, N, a,
         s.precision);
     launched(K_BIN);
     s.pc = np;
@@ -637,7 +651,7 @@ void run_distribute(State& s) {
     s.ac = na;
     if (s.G > 0) {
         k_ghost_links<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.slot_of_ref, s.bsrc_ref, s.broot_ref,
-                                                               s.bcode, s.gsrc, s.groot, s.gcode, N, s.G);
+                                                               s.bcode, s.gsrc, s.groot, s.gcode, s.rref, N, s.G);
         launched(K_BIN);
     }
     prof_end(K_BIN);
@@ -671,12 +685,15 @@ int run_build_lists(State& s, bool half, double cutoff) {
         TMD_CUDA(cudaMemsetAsync(&s.status_dev->bad_code, 0, sizeof(int), s.stream));
         prof_begin(K_NLIST);
         const int nb = nblocks(g.ncells, kNlWarps);
-        if (half)
-            k_build_list<true><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                   s.nbn, s.nbl, s.status_dev, a);
+        if (half && s.half_ghost)
+            k_build_list<2><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart,
+                                                                s.nbn, s.nbl, s.status_dev, a);
+        else if (half)
+            k_build_list<1><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                s.nbn, s.nbl, s.status_dev, a);
         else
-            k_build_list<false><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                    s.nbn, s.nbl, s.status_dev, a);
+            k_build_list<0><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                s.nbn, s.nbl, s.status_dev, a);
         launched(K_NLIST);
         prof_end(K_NLIST);
         TMD_CUDA(cudaMemcpyAsync(s.status_host, s.status_dev, sizeof(DevStatus), cudaMemcpyDeviceToHost, s.stream));

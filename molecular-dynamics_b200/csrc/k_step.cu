@@ -56,42 +56,87 @@ __device__ __forceinline__ void put_partial(double* part, int q, double v, doubl
     if (threadIdx.x == 0) part[q * gridDim.x + blockIdx.x] = r;
 }
 
+// ---- list prefetch ---------------------------------------------------------------
+// Issues one bulk L2 prefetch per list row the block will read (the block's
+// 256 atoms are one contiguous 1 KiB segment of each row of the atom-fastest
+// list), so the whole list tile is in flight before the neighbour loop.
+__device__ __forceinline__ void prefetch_list_rows(const uint32_t* nbl, int n, int stride, int nbcap) {
+    __shared__ int s_rows;
+    if (threadIdx.x == 0) s_rows = 0;
+    __syncthreads();
+    if (n > 0) atomicMax(&s_rows, min(n, nbcap));
+    __syncthreads();
+    const int base = blockIdx.x * blockDim.x;
+    const int cols = min((int)blockDim.x, stride - base);
+    if (cols <= 0) return;
+    for (int r = threadIdx.x; r < s_rows; r += blockDim.x) {
+        const uint32_t* p = nbl + (size_t)r * stride + base;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(cols * 4) : "memory");
+    }
+}
+
+// target of the reaction force of a half-list pair: the local itself or a ghost's root
+__device__ __forceinline__ int reaction_slot(int j, int N, const int* groot) { return j < N ? j : groot[j - N]; }
+
 // ---- FP64 LJ ------------------------------------------------------------------
+#ifndef TMD_B64
+#define TMD_B64 4
+#endif
+#ifndef TMD_B32
+#define TMD_B32 8
+#endif
+#ifndef TMD_MINB
+#define TMD_MINB 1
+#endif
+constexpr int kB64 = TMD_B64;  // neighbours loaded per batch (FP64)
+constexpr int kB32 = TMD_B32;  // neighbours loaded per batch (mixed)
+
 template <bool HALF, bool FUSE, bool THERMO>
 __global__ void __launch_bounds__(kThreads)
 k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* __restrict__ vel,
-          const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, double* __restrict__ part, LjArgs a) {
+          const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot,
+          double* __restrict__ part, LjArgs a) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
+    prefetch_list_rows(nbl, n, a.stride, a.nbcap);
     double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
     if (i < a.N) {
         const double4 pi = pos[i];
-        const int n = min(nbn[i], a.nbcap);
         double fx = 0.0, fy = 0.0, fz = 0.0;
         const uint32_t* lp = nbl + i;
-#pragma unroll 4
-        for (int k = 0; k < n; ++k) {
-            const int j = (int)(__ldg(lp + (size_t)k * a.stride) >> kCodeBits);
-            const double4 pj = ldg_d4(pos + j);
-            const double dx = dsub(pi.x, pj.x), dy = dsub(pi.y, pj.y), dz = dsub(pi.z, pj.z);
-            const double rsq = len2_strict(dx, dy, dz);
-            if (rsq < a.rc2) {
-                const double sr2 = ddiv(1.0, rsq);
-                const double sr6 = dmul(dmul(dmul(sr2, sr2), sr2), a.sigma6);
-                const double f = dmul(dmul(dmul(dmul(48.0, sr6), dsub(sr6, 0.5)), sr2), a.eps);
-                const double px = dmul(dx, f), py = dmul(dy, f), pz = dmul(dz, f);
-                fx = dadd(fx, px);
-                fy = dadd(fy, py);
-                fz = dadd(fz, pz);
-                if (HALF && j < a.N) {
-                    atomicAdd(&frc[j].x, -px);
-                    atomicAdd(&frc[j].y, -py);
-                    atomicAdd(&frc[j].z, -pz);
-                }
-                if (THERMO) {
-                    e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
-                    w += f * rsq;
-                    cnt += 1.0;
+        for (int k0 = 0; k0 < n; k0 += kB64) {
+            int j[kB64];
+            double4 pj[kB64];
+#pragma unroll
+            for (int u = 0; u < kB64; ++u)
+                j[u] = (k0 + u < n) ? (int)(__ldg(lp + (size_t)(k0 + u) * a.stride) >> kCodeBits) : i;
+#pragma unroll
+            for (int u = 0; u < kB64; ++u) pj[u] = ldg_d4(pos + j[u]);
+#pragma unroll
+            for (int u = 0; u < kB64; ++u) {
+                if (k0 + u >= n) continue;
+                const double dx = dsub(pi.x, pj[u].x), dy = dsub(pi.y, pj[u].y), dz = dsub(pi.z, pj[u].z);
+                const double rsq = len2_strict(dx, dy, dz);
+                if (rsq < a.rc2) {
+                    const double sr2 = ddiv(1.0, rsq);
+                    const double sr6 = dmul(dmul(dmul(sr2, sr2), sr2), a.sigma6);
+                    const double f = dmul(dmul(dmul(dmul(48.0, sr6), dsub(sr6, 0.5)), sr2), a.eps);
+                    const double px = dmul(dx, f), py = dmul(dy, f), pz = dmul(dz, f);
+                    fx = dadd(fx, px);
+                    fy = dadd(fy, py);
+                    fz = dadd(fz, pz);
+                    if (HALF) {
+                        const int t = reaction_slot(j[u], a.N, groot);
+                        atomicAdd(&frc[t].x, -px);
+                        atomicAdd(&frc[t].y, -py);
+                        atomicAdd(&frc[t].z, -pz);
+                    }
+                    if (THERMO) {
+                        e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
+                        w += f * rsq;
+                        cnt += 1.0;
+                    }
                 }
             }
         }
@@ -122,40 +167,49 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
 // ---- mixed LJ -----------------------------------------------------------------
 // FP32 pair arithmetic on positions rebased to a dyadic grid of spacing rb_h:
 // del = (r_i - r_j) - dk*rb_h, with dk in {-1,0,1}^3 decoded from the list
-// entry's low bits and the product exact, so del carries one rounding more
-// than r_i - r_j.  Pairs closer than sigma (large forces, ~0.2 per atom in a
-// dense LJ liquid) and pairs within 1e-3 of the cutoff take the FP64 path, so
-// list membership and the cutoff test stay exactly the FP64 decisions.
+// entry's low bits (exact float construction, 3 operations per axis) and the
+// product exact, so del carries one rounding more than r_i - r_j.  Pairs
+// closer than sigma (large forces, ~0.2 per atom in a dense LJ liquid) and
+// pairs within 1e-3 of the cutoff take the FP64 path, so list membership and
+// the cutoff test stay exactly the FP64 decisions.
 template <bool HALF, bool FUSE, bool THERMO>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, TMD_MINB)
 k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
            double4* __restrict__ vel, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
-           double* __restrict__ part, LjArgs a) {
+           const int* __restrict__ groot, double* __restrict__ part, LjArgs a) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
+    prefetch_list_rows(nbl, n, a.stride, a.nbcap);
     double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
     if (i < a.N) {
         const float4 ri = pos32[i];
-        const int n = min(nbn[i], a.nbcap);
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
         const uint32_t* lp = nbl + i;
-#pragma unroll 4
-        for (int k = 0; k < n; ++k) {
-            const uint32_t ent = __ldg(lp + (size_t)k * a.stride);
-            const int j = (int)(ent >> kCodeBits);
-            const float4 rj = __ldg(pos32 + j);
-            const float sx = __int_as_float((int)((ent & 0x03u) | 0x4B000000u)) - 8388609.0f;
-            const float sy = __int_as_float((int)((ent & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
-            const float sz = __int_as_float((int)((ent & 0x30u) | 0x4B000000u)) - 8388624.0f;
-            const float dx = fmaf(a.hx, sx, ri.x - rj.x);
-            const float dy = fmaf(a.hy, sy, ri.y - rj.y);
-            const float dz = fmaf(a.hz, sz, ri.z - rj.z);
-            const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            if (rsq < a.rc2_hi) {
-                bool near = rsq >= a.rc2_lo || rsq < a.close2;
-                if (!near) {
+        for (int k0 = 0; k0 < n; k0 += kB32) {
+            uint32_t ent[kB32];
+            float4 rj[kB32];
+#pragma unroll
+            for (int u = 0; u < kB32; ++u)
+                ent[u] = (k0 + u < n) ? __ldg(lp + (size_t)(k0 + u) * a.stride) : ((uint32_t)i << kCodeBits) | 21u;
+#pragma unroll
+            for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (ent[u] >> kCodeBits));
+#pragma unroll
+            for (int u = 0; u < kB32; ++u) {
+                if (k0 + u >= n) continue;
+                const uint32_t en = ent[u];
+                const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
+                const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
+                const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
+                const float dx = fmaf(a.hx, sx, ri.x - rj[u].x);
+                const float dy = fmaf(a.hy, sy, ri.y - rj[u].y);
+                const float dz = fmaf(a.hz, sz, ri.z - rj[u].z);
+                const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                if (!(rsq < a.rc2_hi)) continue;
+                const int j = (int)(en >> kCodeBits);
+                if (rsq < a.rc2_lo && rsq >= a.close2) {
                     const float sr2 = __frcp_rn(rsq);
                     const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
                     const float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
@@ -163,10 +217,11 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                     fx += px;
                     fy += py;
                     fz += pz;
-                    if (HALF && j < a.N) {
-                        atomicAdd(&frc32[j].x, -px);
-                        atomicAdd(&frc32[j].y, -py);
-                        atomicAdd(&frc32[j].z, -pz);
+                    if (HALF) {
+                        const int t = reaction_slot(j, a.N, groot);
+                        atomicAdd(&frc32[t].x, -px);
+                        atomicAdd(&frc32[t].y, -py);
+                        atomicAdd(&frc32[t].z, -pz);
                     }
                     if (THERMO) {
                         ef += a.eps4f * sr6 * (sr6 - 1.0f);
@@ -186,10 +241,11 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                         cx += ex * f;
                         cy += ey * f;
                         cz += ez * f;
-                        if (HALF && j < a.N) {
-                            atomicAdd(&frc32[j].x, (float)(-ex * f));
-                            atomicAdd(&frc32[j].y, (float)(-ey * f));
-                            atomicAdd(&frc32[j].z, (float)(-ez * f));
+                        if (HALF) {
+                            const int t = reaction_slot(j, a.N, groot);
+                            atomicAdd(&frc32[t].x, (float)(-ex * f));
+                            atomicAdd(&frc32[t].y, (float)(-ey * f));
+                            atomicAdd(&frc32[t].z, (float)(-ez * f));
                         }
                         if (THERMO) {
                             e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
@@ -279,7 +335,7 @@ __device__ __forceinline__ void dem_pair(const double4& del, double rsq, const d
 template <bool HALF>
 __global__ void __launch_bounds__(kThreads)
 k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, double4* __restrict__ frc,
-           const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, DemArgs a) {
+           const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot, DemArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.N) return;
     const double4 pi = pos[i];
@@ -297,10 +353,11 @@ k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, dou
             F[0] = dadd(F[0], f[0]);
             F[1] = dadd(F[1], f[1]);
             F[2] = dadd(F[2], f[2]);
-            if (HALF && j < a.N) {
-                atomicAdd(&frc[j].x, -f[0]);
-                atomicAdd(&frc[j].y, -f[1]);
-                atomicAdd(&frc[j].z, -f[2]);
+            if (HALF) {
+                const int t = reaction_slot(j, a.N, groot);
+                atomicAdd(&frc[t].x, -f[0]);
+                atomicAdd(&frc[t].y, -f[1]);
+                atomicAdd(&frc[t].z, -f[2]);
             }
         }
     }
@@ -496,10 +553,10 @@ void launch_lj(State& s, const LjArgs& a, int nb) {
     double4* vel = s.vel.b[s.vc];
     if (s.precision == 1)
         k_lj_mixed<HALF, FUSE, THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos32, s.pos.b[s.pc], s.frc32, vel, s.nbn,
-                                                                     s.nbl, s.red_part, a);
+                                                                     s.nbl, s.groot, s.red_part, a);
     else
         k_lj_fp64<HALF, FUSE, THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn, s.nbl,
-                                                                    s.red_part, a);
+                                                                    s.groot, s.red_part, a);
 }
 
 }  // namespace
@@ -597,10 +654,10 @@ void run_force_dem(State& s, const PendingForce& p) {
     prof_begin(K_FORCE_DEM);
     if (p.half)
         k_dem_fp64<true><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc],
-                                                                          s.frc.b[s.ac], s.nbn, s.nbl, a);
+                                                                          s.frc.b[s.ac], s.nbn, s.nbl, s.groot, a);
     else
         k_dem_fp64<false><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc],
-                                                                           s.frc.b[s.ac], s.nbn, s.nbl, a);
+                                                                           s.frc.b[s.ac], s.nbn, s.nbl, s.groot, a);
     launched(K_FORCE_DEM);
     prof_end(K_FORCE_DEM);
 }

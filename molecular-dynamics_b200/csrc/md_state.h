@@ -70,6 +70,7 @@ struct State {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    bool stream_set = false;   // a caller chose the stream (md_set_stream), NULL included
     Geometry geo{};
 
     // sizes
@@ -84,6 +85,7 @@ struct State {
     // modes
     int precision = 0;   // 0 FP64, 1 mixed
     int ghost_exact = 0;
+    int half_ghost = 0;  // half lists keep local-ghost pairs (ordered by root) -- corrected half mode
     int dem_fixed = 0;
     double dem_radius = 1.0;
     int thermo = 0;
@@ -96,6 +98,7 @@ struct State {
     float4* pos32 = nullptr;   // mixed-form rebased positions
     int* rbk = nullptr;        // packed rebasing cell of each slot
     int* slot_of_ref = nullptr;
+    int* rref = nullptr;       // per slot: reference index of the root local (= ref for locals)
     int* gsrc = nullptr;       // ghost: source slot (reference two-phase refresh)
     int* groot = nullptr;      // ghost: root local slot
     int* gcode = nullptr;      // ghost: shifts (see md_common.cuh)
@@ -130,6 +133,7 @@ struct State {
     std::vector<double> h_x0;                   // initial positions (adjoint)
 
     PendingForce pend_force;
+    PendingForce force_cfg;   // parameters of the last md_compute_* call
     bool pend_init = false;
     double pend_dt = 0.0;
 

@@ -10,6 +10,7 @@
 #ifdef TINYMD_DRIVER_CPU_ORACLE
 extern "C" {
 void oracle_set_ghost_mode(int exact);
+void oracle_set_half_mode(int ghost_pairs);
 void oracle_set_dem_mode(int contact_fixed, double radius);
 void oracle_set_threads(int n);
 int oracle_max_threads(void);
@@ -20,6 +21,7 @@ namespace drv {
 constexpr bool kGpu = false;
 inline void set_precision(int) {}
 inline void set_ghost_mode(int exact) { oracle_set_ghost_mode(exact); }
+inline void set_half_mode(int g) { oracle_set_half_mode(g); }
 inline void set_dem_model(int fixed, double radius) { oracle_set_dem_mode(fixed, radius); }
 inline void set_threads(int n) { oracle_set_threads(n); }
 inline void set_thermo(int) {}
@@ -41,6 +43,7 @@ namespace drv {
 constexpr bool kGpu = true;
 inline void set_precision(int m) { md_set_precision(m); }
 inline void set_ghost_mode(int exact) { md_set_ghost_mode(exact); }
+inline void set_half_mode(int g) { md_set_half_mode(g); }
 inline void set_dem_model(int fixed, double radius) { md_set_dem_model(fixed, radius); }
 inline void set_threads(int) {}
 inline void set_thermo(int on) { md_set_thermo(on); }

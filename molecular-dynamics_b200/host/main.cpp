@@ -94,6 +94,7 @@ void usage(const char* name) {
               << "\t    --prebalance          static load balancing before the run (accepted; single process)\n"
               << "\t    --precision=STRING    fp64 (default) or mixed (FP32 pair forces)\n"
               << "\t    --ghost=STRING        reference (default, two-phase ghost refresh) or exact\n"
+              << "\t    --half_mode=STRING    reference (default: half lists drop periodic-boundary pairs) or ghost\n"
               << "\t    --dem_model=STRING    reference (default) or fixed (contact-fixed spring-dashpot)\n"
               << "\t    --dem_radius=REAL     contact radius of the fixed DEM model (default cutoff/2)\n"
               << "\t    --thermo=NUMBER       print a thermo line every NUMBER steps (0 = off)\n"
@@ -168,13 +169,13 @@ int main(int argc, char** argv) {
     double dt = 0.005, cutoff = 2.5, verlet = 0.3, epsilon = 1.0, sigma = 1.0, potmin = 1.6796, init_temp = 1.44;
     double damping_n = 0.0, damping_t = 0.0, stiffness = 0.0, friction = 0.0;
     bool half_nb = false, prebalance = false, perf = false;
-    std::string precision = "fp64", ghost = "reference", dem_model = "reference";
+    std::string precision = "fp64", ghost = "reference", dem_model = "reference", half_mode = "reference";
     double dem_radius = -1.0;
     int thermo_every = 0;
 
     enum {
         O_RENEIGH = 256, O_REBALANCE, O_DT, O_TEMP, O_CUTOFF, O_VERLET, O_EPS, O_SIGMA, O_DN, O_DT_, O_K, O_MU,
-        O_POTMIN, O_HALF, O_PREBAL, O_PREC, O_GHOST, O_DEMMODEL, O_DEMR, O_THERMO, O_PERF
+        O_POTMIN, O_HALF, O_PREBAL, O_PREC, O_GHOST, O_DEMMODEL, O_DEMR, O_THERMO, O_PERF, O_HALFMODE
     };
     static option opts[] = {{"force_field", required_argument, nullptr, 'f'},
                             {"benchmark", required_argument, nullptr, 'b'},
@@ -208,6 +209,7 @@ int main(int argc, char** argv) {
                             {"dem_radius", required_argument, nullptr, O_DEMR},
                             {"thermo", required_argument, nullptr, O_THERMO},
                             {"perf", no_argument, nullptr, O_PERF},
+                            {"half_mode", required_argument, nullptr, O_HALFMODE},
                             {nullptr, 0, nullptr, 0}};
     int opt;
     while ((opt = getopt_long(argc, argv, "f:b:x:y:z:s:r:t:a:v:h", opts, nullptr)) != -1) {
@@ -243,6 +245,7 @@ int main(int argc, char** argv) {
             case O_DEMR: dem_radius = std::atof(optarg); break;
             case O_THERMO: thermo_every = std::atoi(optarg); break;
             case O_PERF: perf = true; break;
+            case O_HALFMODE: half_mode = optarg; break;
             default: usage(argv[0]); return EXIT_FAILURE;
         }
     }
@@ -276,6 +279,7 @@ int main(int argc, char** argv) {
 
     drv::set_precision(precision == "mixed" ? 1 : 0);
     drv::set_ghost_mode(ghost == "exact" ? 1 : 0);
+    drv::set_half_mode(half_mode == "ghost" ? 1 : 0);
     drv::set_dem_model(dem_model == "fixed" ? 1 : 0, dem_radius > 0 ? dem_radius : 0.5 * cutoff);
     drv::set_threads(nthreads);
     drv::set_thermo(thermo_every > 0 ? 1 : 0);

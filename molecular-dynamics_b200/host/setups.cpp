@@ -140,7 +140,9 @@ int generate(int benchmark, const double world[6], const double rank[6], const d
             fcc_walk(world, spacing, false,
                      [&](const Vector3D& p, const int*, const int*) {
                          if (!inside_rank(rank, p.x, p.y, p.z)) return false;
-                         return (p.x - world[0]) / lx + (p.y - world[2]) / ly < 1.0;
+                         // strictly below the diagonal; the tolerance keeps sites that lie
+                         // on it (i + j = sites per edge) out regardless of rounding
+                         return (p.x - world[0]) / lx + (p.y - world[2]) / ly < 1.0 - 1e-9;
                      },
                      out);
             break;

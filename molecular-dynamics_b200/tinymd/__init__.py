@@ -65,6 +65,7 @@ _EXTENSION_API = {
     "md_clear_error": (None, []),
     "md_set_precision": (None, [_c_int]),
     "md_set_ghost_mode": (None, [_c_int]),
+    "md_set_half_mode": (None, [_c_int]),
     "md_set_dem_model": (None, [_c_int, _c_double]),
     "md_set_thermo": (None, [_c_int]),
     "md_get_thermo": (_c_int, [_vp]),
@@ -85,6 +86,7 @@ _EXTENSION_API = {
     "md_set_velocities": (_c_int, [_vp]),
     "md_get_cell_sizes": (_c_int, [_vp, _c_int]),
     "md_get_grid_info": (_c_int, [_vp]),
+    "md_run_timesteps": (_c_int, [_c_int, _c_double, _c_int, _c_int, _c_double, _vp, _vp, _c_ll]),
     "tmd_setup_world": (_c_int, [_c_int, _vp, _c_double, _vp, _vp, _vp]),
     "tmd_setup_rank_box": (None, [_vp, _vp]),
     "tmd_setup_generate": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_double]),
@@ -98,6 +100,7 @@ _EXTENSION_API = {
 
 _ORACLE_API = {
     "oracle_set_ghost_mode": (None, [_c_int]),
+    "oracle_set_half_mode": (None, [_c_int]),
     "oracle_set_dem_mode": (None, [_c_int, _c_double]),
     "oracle_set_threads": (None, [_c_int]),
     "oracle_max_threads": (_c_int, []),
@@ -241,6 +244,19 @@ class Simulation:
         lib.md_borders()
         lib.md_distribute_particles()
         lib.md_assemble_neighborlists(self.half, self.cell)
+
+    def run(self, dt, steps, step_ms=None, flush=None):
+        """`steps` timesteps issued natively by md_run_timesteps (product library only).
+
+        step_ms: float32 array receiving per-step device times; flush: (pointer, bytes)
+        of a device buffer overwritten before each step (outside the timed interval)."""
+        fp, fb = (flush if flush is not None else (None, 0))
+        rc = self.lib.md_run_timesteps(steps, dt, self.reneigh, self.step_count, self.cell,
+                                       ptr(step_ms), fp, fb)
+        check(self.lib)
+        if rc != 0:
+            raise MDError("md_run_timesteps failed")
+        self.step_count += steps
 
     def step(self, dt, steps=1):
         """`steps` timesteps of main.cpp:715-776."""

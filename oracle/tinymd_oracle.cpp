@@ -75,6 +75,7 @@ bool g_alive = false;
 int64_t force_iters = 0, rsq_iters = 0, integration_iters = 0;
 int ghost_exact = 0;        // 0 = reference two-phase (lagged) ghost update
 int dem_contact_fixed = 0;  // 0 = reference DEM closure (contact branch unreachable)
+int half_ghost = 0;         // 1 = corrected half lists: local-ghost pairs kept by root order
 double dem_radius = 1.0;    // core/runtime.impala:210 hard-codes 1.0
 
 // thermo extension: last LJ potential energy sum / virial sum over list pairs
@@ -382,7 +383,10 @@ void assemble_neighborlists(int half, double cutoff) {
                         for (int k = 0; k < size; ++k) {
                             int j = cp[k];
                             if (chk && i == j) continue;
-                            if (half != 0 && !(i > j)) continue;
+                            // core/neighborlist.impala:34; the corrected mode orders a
+                            // ghost by its root local so boundary pairs are kept once
+                            const int jo = (half_ghost && j >= g.nparticles) ? c.root[j - g.nparticles] : j;
+                            if (half != 0 && !(i > jo)) continue;
                             const double* pj = P(g.pos, j);
                             double dx = pi[0] - pj[0];
                             double dy = pi[1] - pj[1];
@@ -437,8 +441,9 @@ void compute_lj(int half, double rc, double eps, double sigma) {
                     double fx = dx * f, fy = dy * f, fz = dz * f;
                     double* Fi = P(g.force, i);
                     Fi[0] += fx; Fi[1] += fy; Fi[2] += fz;
-                    if (j < N) {
-                        double* Fj = P(g.force, j);
+                    const int jt = j < N ? j : (half_ghost ? c.root[j - N] : -1);
+                    if (jt >= 0) {
+                        double* Fj = P(g.force, jt);
                         Fj[0] += -fx; Fj[1] += -fy; Fj[2] += -fz;
                     }
                     epot += 4.0 * eps * sr6 * (sr6 - 1.0);
@@ -549,8 +554,9 @@ void compute_dem(int half, double rc, double dn, double dt_, double k, double mu
                     dem_pair(i, j, del, rsq, dn, dt_, k, mu, f);
                     double* Fi = P(g.force, i);
                     Fi[0] += f[0]; Fi[1] += f[1]; Fi[2] += f[2];
-                    if (j < N) {
-                        double* Fj = P(g.force, j);
+                    const int jt = j < N ? j : (half_ghost ? c.root[j - N] : -1);
+                    if (jt >= 0) {
+                        double* Fj = P(g.force, jt);
                         Fj[0] += -f[0]; Fj[1] += -f[1]; Fj[2] += -f[2];
                     }
                     inside++;
@@ -782,6 +788,7 @@ void md_deallocate_grid(void) {
 
 // ---- oracle_* introspection (tests only) ---------------------------------
 void oracle_set_ghost_mode(int exact) { ghost_exact = exact; }
+void oracle_set_half_mode(int ghost_pairs) { half_ghost = ghost_pairs ? 1 : 0; }
 void oracle_set_dem_mode(int contact_fixed, double radius) {
     dem_contact_fixed = contact_fixed;
     dem_radius = radius;

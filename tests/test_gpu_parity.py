@@ -129,3 +129,69 @@ def test_mixed_force_error(product, oracle):
     finally:
         product.md_set_precision(0)
         p.close()
+
+
+def test_half_lists_with_ghost_pairs(product, oracle):
+    """Corrected half mode: lists equal the oracle's; forces equal the full-list forces."""
+    product.md_set_half_mode(1)
+    oracle.oracle_set_half_mode(1)
+    try:
+        p, o = both(product, oracle, cells=(8, 8, 8), half=True)
+        try:
+            lp = tinymd.neighbor_lists(product, p.n)
+            lo = tinymd.neighbor_lists(oracle, o.n)
+            for a, b in zip(lp, lo):
+                np.testing.assert_array_equal(a, b)
+            _, _, fp = tinymd.full_state(product)
+            _, _, fo = tinymd.full_state(oracle)
+            assert rel_err(fp, fo) < 1e-12
+            p.step(0.005, 45)
+            o.step(0.005, 45)
+            xp, _, fp = tinymd.full_state(product)
+            xo, _, fo = tinymd.full_state(oracle)
+            assert rel_err(xp, xo) < 1e-10 and rel_err(fp, fo) < 1e-9
+        finally:
+            close_all(p, o)
+        # same physics as the full list (exact periodic ghosts keep pair forces symmetric)
+        product.md_set_ghost_mode(1)
+        f = make_sim(product, setup_lib=product, cells=(8, 8, 8))
+        f.step(0.005, 25)
+        _, _, ffull = tinymd.full_state(product)
+        f.close()
+        h = make_sim(product, setup_lib=product, cells=(8, 8, 8), half=True)
+        h.step(0.005, 25)
+        _, _, fhalf = tinymd.full_state(product)
+        h.close()
+        assert rel_err(fhalf, ffull) < 1e-10
+    finally:
+        product.md_set_half_mode(0)
+        product.md_set_ghost_mode(0)
+        oracle.oracle_set_half_mode(0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_131k_workload_stable_and_matches_oracle_lists(product, oracle, precision):
+    """The benchmark workload: lists equal the oracle's after reneighbouring; energy stays bounded."""
+    product.md_set_precision(precision)
+    try:
+        p = make_sim(product, setup_lib=product, cells=(32, 32, 32))
+        o = make_sim(oracle, setup_lib=product, cells=(32, 32, 32))
+        p.step(0.005, 20)
+        o.step(0.005, 20)
+        lp = tinymd.neighbor_lists(product, p.n)
+        lo = tinymd.neighbor_lists(oracle, o.n)
+        if precision == 0:
+            for a, b in zip(lp, lo):
+                np.testing.assert_array_equal(a, b)
+            xp, vp, _ = tinymd.full_state(product)
+            xo, vo, _ = tinymd.full_state(oracle)
+            np.testing.assert_array_equal(xp, xo)
+        o.close()
+        p.run(0.005, 380)
+        _, v, _ = tinymd.full_state(product)
+        t = float((v ** 2).sum() / (3 * p.n - 3))
+        assert 0.5 < t < 1.2, t
+        assert product.md_last_error() == 0
+        p.close()
+    finally:
+        product.md_set_precision(0)
