@@ -271,7 +271,9 @@ def run_ours(args):
     value64 = total_atoms * K / (ms64 * 1e-3)
     peak, peak_kind = peaks()
     force_ms = fms.value / max(nl.value, 1)
-    bytes_per_atom = 4 + mean_nb * (4 + 16) + 16 + 16  # count, list entry + float4 gather, own float4 pos, float4 force
+    # algorithmic bytes per atom and force launch (payload only, padding excluded): the list
+    # count, per neighbour a 4-byte index and a 12-byte FP32 position, own FP32 position, FP32 force
+    bytes_per_atom = 4 + mean_nb * (4 + 12) + 12 + 12
     achieved = natoms * bytes_per_atom / (force_ms * 1e-3) / 1e9
     traffic = measured_traffic()
     line = {
@@ -312,6 +314,22 @@ def run_ours(args):
 import ctypes  # noqa: E402
 
 
+def profile_case(args):
+    """The benchmark workload in one form for `args.steps` steps, untimed (an ncu target)."""
+    import tinymd as tm
+    lib = tm.load()
+    half = args.profile_case.endswith("_half")
+    lib.md_set_precision(1 if args.profile_case.startswith("mixed") else 0)
+    if half:
+        lib.md_set_half_mode(1)
+        lib.md_set_ghost_mode(1)
+    sim = tm.Simulation(lib, *tm.setup_particles("default", CELLS, lib=lib), temp=1.44, half=half)
+    sim.run(DT, args.steps)
+    sim.close()
+    print(f"profile case {args.profile_case}: {args.steps} steps, error code {lib.md_last_error()}")
+    return 0 if lib.md_last_error() == 0 else 1
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,7 +337,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", choices=["mixed", "fp64", "mixed_half", "fp64_half"],
+                    help="run the workload for --steps steps in one form and exit (for ncu captures)")
     args = ap.parse_args()
+    if args.profile_case:
+        return profile_case(args)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

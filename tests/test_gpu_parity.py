@@ -144,7 +144,7 @@ def test_half_lists_with_ghost_pairs(product, oracle):
                 np.testing.assert_array_equal(a, b)
             _, _, fp = tinymd.full_state(product)
             _, _, fo = tinymd.full_state(oracle)
-            assert rel_err(fp, fo) < 1e-12
+            assert np.abs(fp - fo).max() < 1e-12  # perfect lattice: forces are rounding noise
             p.step(0.005, 45)
             o.step(0.005, 45)
             xp, _, fp = tinymd.full_state(product)
