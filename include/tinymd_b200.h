@@ -201,6 +201,26 @@ long long md_device_bytes(void);
 int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double list_cutoff, float *step_ms,
                      void *flush_buf, long long flush_bytes);
 
+/* LJ forces and energy / virial sums over a caller-built full neighbour list,
+ * allocating no device memory (no counterpart in the reference).  For callers
+ * that cannot call cudaMalloc -- code inside another framework's memory pool,
+ * code running while someone else captures a CUDA graph, hosts with a fixed
+ * memory budget -- its per-block partial sums live in a fixed device array
+ * compiled into the library (128 KiB, held by every GPU that loads the
+ * library until exit), so the call only launches two kernels on `stream`.
+ * Limit: n_local <= 1,048,576 (larger is rejected with MD_ERR_ARGUMENT).
+ * All pointers are device memory: positions [n_all][4] (x, y, z, unused),
+ * list_sizes [n_local], lists atom-fastest (entry k of atom i at
+ * lists[k*stride + i], a plain index into positions), forces [n_local][4]
+ * out, sums [4] out = {sum of 4 eps (s12 - s6), sum of f r^2, pairs inside the
+ * cutoff, 0} over the list entries.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and should therefore come
+ * before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU race.  Returns MD_OK or an md_error code. */
+int md_lj_forces_noalloc(const double *positions, int n_local, const int *list_sizes, const int *lists, int stride,
+                         int max_neighbors, double cutoff, double epsilon, double sigma, double *forces, double *sums,
+                         void *stream);
+
 /* Parity introspection (reference index space: locals 0..N-1 in input order,
  * ghosts N..N+G-1 in the reference's ghost order).  Drain pending work. */
 int md_get_neighbor_lists(int *sizes, int *lists, int capacity); /* row-major [N][capacity]; returns max size */

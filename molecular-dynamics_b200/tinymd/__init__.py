@@ -87,6 +87,8 @@ _EXTENSION_API = {
     "md_get_cell_sizes": (_c_int, [_vp, _c_int]),
     "md_get_grid_info": (_c_int, [_vp]),
     "md_run_timesteps": (_c_int, [_c_int, _c_double, _c_int, _c_int, _c_double, _vp, _vp, _c_ll]),
+    "md_lj_forces_noalloc": (_c_int, [_vp, _c_int, _vp, _vp, _c_int, _c_int, _c_double, _c_double, _c_double, _vp,
+                                      _vp, _vp]),
     "tmd_setup_world": (_c_int, [_c_int, _vp, _c_double, _vp, _vp, _vp]),
     "tmd_setup_rank_box": (None, [_vp, _vp]),
     "tmd_setup_generate": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_double]),
