@@ -20,6 +20,11 @@ roofline  the mixed force kernel: algorithmic bytes per launch / average
         measured HBM bandwidth.
 cpu_baseline  the CPU oracle (a restatement of the reference's cpu backend)
         timed on this host over a bounded sample of the same workload.
+drift   total energy per atom over 1000 steps of the workload, sampled every
+        50 steps, in both forms (max |E(t) - E(0)| / N and the ratio).
+adjoint the differentiable form on 16x16x16 cells (16,384 atoms), 200 steps,
+        checkpoints every 20 steps: device time of the backward pass over the
+        forward pass.
 
 --impl reference runs that CPU path alone (all host threads) on the same
 workload and prints the same JSON line.  Under torchrun each rank runs an
@@ -46,6 +51,8 @@ UNIT = "atom-steps/s"
 CELLS = (32, 32, 32)
 DT = 0.005
 L2_FLUSH_BYTES = 256 << 20
+DRIFT_STEPS = 1000
+DRIFT_EVERY = 50
 
 
 def peaks():
@@ -195,6 +202,56 @@ def timed_steps(lib, sim, steps, flush):
     return float(step_ms.astype(np.float64).sum()), lib.md_kernel_launches() - launches0
 
 
+def energy_drift(lib, tm, parts, precision):
+    """Total energy per atom, (KE + U) / N with U from the full list, sampled every
+    DRIFT_EVERY steps over DRIFT_STEPS steps of the benchmark workload in one form."""
+    lib.md_set_precision(precision)
+    lib.md_set_thermo(1)
+    sim = tm.Simulation(lib, *parts, temp=1.44)
+    n = len(parts[0])
+    t = np.zeros(4)
+    series = []
+    for k in range(DRIFT_STEPS // DRIFT_EVERY + 1):
+        if k:
+            sim.run(DT, DRIFT_EVERY)
+        else:  # step 0: forces and kinetic energy of the initial state
+            sim.force()
+            lib.md_final_integration(0.0)
+        if lib.md_get_thermo(tm.ptr(t)) != 0:
+            tm.check(lib)
+        series.append((0.5 * t[3] + 0.5 * t[0]) / n)  # t = {U sum, virial, pairs, v.v}
+    sim.close()
+    lib.md_set_thermo(0)
+    lib.md_set_precision(0)
+    e = np.array(series)
+    return {"e0_per_atom": float(e[0]), "max_abs_drift_per_atom": float(np.max(np.abs(e - e[0]))),
+            "end_drift_per_atom": float(e[-1] - e[0])}
+
+
+def adjoint_times(lib, tm):
+    """Differentiable form on its own workload: 16x16x16 cells (16,384 atoms), 200 steps of dt
+    0.005, checkpoints every 20 steps, mixed forward; device ms of one forward and one backward
+    pass (after one untimed pass of each)."""
+    import torch
+    from tinymd import adjoint
+    parts = tm.setup_particles("default", (16, 16, 16), lib=lib)
+    sim = tm.Simulation(lib, *parts, temp=1.44)
+    v0 = adjoint.initial_velocities(lib, sim)
+    adjoint.configure(lib, steps=200, reneigh=20, dt=DT, precision=1, shifted_energy=True)
+    rows = []
+    for _ in range(2):
+        v = torch.tensor(v0, requires_grad=True)
+        e = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+        s = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+        adjoint.TrajectoryLoss.apply(v, e, s, lib).backward()
+        rows.append(adjoint.times(lib))
+    sim.close()
+    fwd, bwd = rows[-1]
+    return {"workload": "lj_default_fcc_16x16x16_16384_atoms_200_steps_checkpoint_20", "forward_ms": fwd,
+            "backward_ms": bwd, "backward_over_forward": bwd / fwd,
+            "loss": "MSD + shifted U(x_T)/N; grads wrt eps, sigma, all initial velocities"}
+
+
 def run_ours(args):
     import torch
     import tinymd as tm
@@ -247,6 +304,13 @@ def run_ours(args):
     sim.close()
     ms32 = allreduce_max(ms32, dist, dev)
 
+    drift = {"steps": DRIFT_STEPS, "every": DRIFT_EVERY}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        drift[name] = energy_drift(lib, tm, parts, prec)
+    drift["mixed_over_fp64"] = drift["mixed"]["max_abs_drift_per_atom"] / max(
+        drift["fp64"]["max_abs_drift_per_atom"], 1e-300)
+    adj = adjoint_times(lib, tm)
+
     # ---- end to end through the C ABI with host buffers ---------------------------
     lib.md_set_precision(1)
     m, x, v, world_box, rank_box = parts
@@ -293,6 +357,8 @@ def run_ours(args):
         "e2e": {"value": total_atoms * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
                 "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock"},
+        "drift": drift,
+        "adjoint": adj,
         "gpu_launches": int(launches),
         "clocks": clocks,
     }

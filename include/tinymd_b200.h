@@ -167,9 +167,9 @@ void md_set_dem_model(int contact_fixed, double radius);
  * and final integrations reduce the kinetic energy (FP64, deterministic). */
 void md_set_thermo(int enable);
 /* out[0] = sum of pair energies 4 eps (s12 - s6) over list entries inside the
- * cutoff, out[1] = sum of f(r) r^2 over the same entries, out[2] = sum of v.v
- * of locals after the last final integration, out[3] = number of list entries
- * inside the cutoff.  Full lists count each pair twice. Returns 0 on success. */
+ * cutoff, out[1] = sum of f(r) r^2 over the same entries, out[2] = number of
+ * list entries inside the cutoff, out[3] = sum of v.v of locals after the last
+ * final integration.  Full lists count each pair twice. Returns 0 on success. */
 int md_get_thermo(double *out);
 /* Blocks until all enqueued device work is done. */
 void md_synchronize(void);
@@ -258,6 +258,10 @@ int md_adjoint_configure(int steps, int reneigh, double dt, double cutoff, doubl
 int md_adjoint_forward(double const *v0, double epsilon, double sigma, double *loss);
 /* Reverse pass: dL/dv0 ([N][3], input order), dL/deps, dL/dsigma. */
 int md_adjoint_backward(double *grad_v0, double *grad_eps, double *grad_sigma);
+/* Loss energy: 0 = U as the reference defines pair energies (unshifted, hard
+ * cutoff: L jumps when a pair crosses the cutoff; default), 1 = U shifted to
+ * zero at the cutoff per pair (continuous in the parameters; same forces). */
+int md_adjoint_set_loss(int shifted_energy);
 /* GPU ms of the last forward and backward passes. */
 int md_adjoint_times(double *forward_ms, double *backward_ms);
 

@@ -1,15 +1,577 @@
-// adjoint.cu -- differentiable form (placeholder until the adjoint kernels land).
+// adjoint.cu -- the differentiable form: gradients of a trajectory loss with
+// respect to the initial velocities, epsilon and sigma by reverse-mode
+// differentiation of velocity-Verlet with LJ over full neighbour lists.
+//
+// Trajectory (the md driver loop, main.cpp:715-776, with exact periodic
+// ghosts): v_h = v_t + c F(x_t); x_{t+1} = x_t + dt v_h; v_{t+1} = v_h + c F(x_{t+1}),
+// c = dt/2, lists rebuilt (after a periodic wrap) whenever (t+1) % R == 0.
+// Loss: L = (1/N) sum_i |x_T,i - x_0,i|^2 (unwrapped) + U(x_T)/N.
+//
+// Reverse pass.  With a_x = dL/dx_t and a_v = dL/dv_t, one step back is
+//   a_x += c J(x_{t+1}) a_v ; a_v += dt a_x ; a_x += c J(x_t) a_v ; (theta: c dF/dtheta^T a_v at both)
+// where J = dF/dx = -Hessian.  The product J(x_t) a_v(t) appears in step t
+// (initial kick) and step t-1 (final kick), so one Hessian-vector product per
+// step suffices: k_adj_hvp computes u = J(x_t) a_v, adds dt*u (c*u at t = 0)
+// to a_x, applies the next drift a_v += dt a_x, and accumulates the theta
+// terms with weight dt (c at t = 0) into per-block sums (deterministic).
+//
+// Memory: a checkpoint (positions, velocities, wrap counts in reference
+// order) per reneighbour segment; the backward pass restores a segment,
+// rebuilds its cells / ghosts / list (bit-identical to the forward's: all are
+// keyed by reference index) and recomputes the segment's positions with the
+// same kernels, so the recomputed trajectory is the forward one bit for bit.
+
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "md_common.cuh"
 #include "md_state.h"
 #include "tinymd_b200.h"
+
+namespace tmd {
+
+void grow_atoms(State& s, int need);
+
+namespace {
+
+constexpr int kT = 256;
+
+struct AdjConfig {
+    bool configured = false;
+    int steps = 0, reneigh = 20, precision = 1;
+    int shifted = 0;  // loss energy shifted to zero at the cutoff (continuous)
+    double dt = 0.005, cutoff = 2.5, skin = 0.3;
+};
+
+struct AdjRun {
+    bool forward_done = false;
+    double eps = 1.0, sigma = 1.0, loss = 0.0, U = 0.0;
+    int nseg = 0;
+    double fwd_ms = 0.0, bwd_ms = 0.0;
+};
+
+AdjConfig cfg;
+AdjRun run;
+
+// device buffers (sized N or N+G)
+double4* ck_x = nullptr;   // [nseg][N] positions, reference order
+double4* ck_v = nullptr;   // [nseg][N] velocities
+int* ck_img = nullptr;     // [nseg][N] wrap counts
+double4* x0_dev = nullptr; // [N] initial positions, reference order
+double4* seg_x = nullptr;  // [reneigh][N] local positions of one segment, slot order
+double4* ax = nullptr;     // [N] adjoint of positions, slot order
+double4* av[2] = {nullptr, nullptr};
+double4* tmp4 = nullptr;   // [N] reference-order staging
+double* gacc = nullptr;    // [3][nblk] per-block theta sums (eps, sigma, unused)
+double* red = nullptr;     // [8] reduced sums
+int cap_n = 0, cap_seg = 0, cap_ck = 0;
+
+inline int nblk(int n) { return (n + kT - 1) / kT; }
+
+struct HvpArgs {
+    int N, stride, nbcap;
+    double rc2, sigma6, eps, inv_sigma;
+    double len[3];
+    double kick;       // added to a_x: dt * u (c * u at t = 0)
+    double drift;      // a_v += drift * a_x after the kick (0 at t = 0)
+    double wt;         // weight of this position's theta terms
+};
+
+// u_i = sum_j [f(s) w_ij + 2 f'(s) (d . w_ij) d],  w_ij = w_i - w_j, d = x_i - x_j,
+// f = 48 eps sr6 (sr6 - 1/2) sr2, f' = df/ds = 48 eps sr2^2 sr6 (2 - 7 sr6);
+// theta terms: w_i . F_i / eps and sum_j df/dsigma (d . w_i),
+// df/dsigma = (144 eps / sigma) sr2 sr6 (4 sr6 - 1).
+__global__ void __launch_bounds__(kT)
+k_adj_hvp(const double4* __restrict__ xs, const double4* __restrict__ w, double4* __restrict__ w_next,
+          double4* __restrict__ ax, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
+          const int* __restrict__ groot, const int* __restrict__ gcode, double* __restrict__ gacc, HvpArgs a) {
+    __shared__ double scratch[kT / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double ge = 0.0, gs = 0.0;
+    if (i < a.N) {
+        const double4 xi = xs[i];
+        const double4 wi = w[i];
+        double ux = 0.0, uy = 0.0, uz = 0.0, Fx = 0.0, Fy = 0.0, Fz = 0.0;
+        const int n = min(nbn[i], a.nbcap);
+        for (int k = 0; k < n; ++k) {
+            const int j = (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits);
+            double4 xj, wj;
+            if (j < a.N) {
+                xj = xs[j];
+                wj = w[j];
+            } else {
+                const int g = j - a.N;
+                const int r = groot[g];
+                const int code = gcode[g];
+                xj = xs[r];
+                xj.x += a.len[0] * shift_axis(code, 8, 0);
+                xj.y += a.len[1] * shift_axis(code, 8, 1);
+                xj.z += a.len[2] * shift_axis(code, 8, 2);
+                wj = w[r];
+            }
+            const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+            const double s = dx * dx + dy * dy + dz * dz;
+            if (s < a.rc2) {
+                const double sr2 = 1.0 / s;
+                const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
+                const double f = 48.0 * a.eps * sr6 * (sr6 - 0.5) * sr2;
+                const double fp = 48.0 * a.eps * sr2 * sr2 * sr6 * (2.0 - 7.0 * sr6);
+                const double wx = wi.x - wj.x, wy = wi.y - wj.y, wz = wi.z - wj.z;
+                const double dw = 2.0 * fp * (dx * wx + dy * wy + dz * wz);
+                ux += f * wx + dw * dx;
+                uy += f * wy + dw * dy;
+                uz += f * wz + dw * dz;
+                Fx += f * dx;
+                Fy += f * dy;
+                Fz += f * dz;
+                gs += 144.0 * a.eps * a.inv_sigma * sr2 * sr6 * (4.0 * sr6 - 1.0) *
+                      (dx * wi.x + dy * wi.y + dz * wi.z);
+            }
+        }
+        ge = (wi.x * Fx + wi.y * Fy + wi.z * Fz) / a.eps;
+        double4 q = ax[i];
+        q.x += a.kick * ux;
+        q.y += a.kick * uy;
+        q.z += a.kick * uz;
+        ax[i] = q;
+        w_next[i] = make_double4(wi.x + a.drift * q.x, wi.y + a.drift * q.y, wi.z + a.drift * q.z, 0.0);
+    }
+    const double se = block_sum(ge, scratch);
+    const double ss = block_sum(gs, scratch);
+    if (threadIdx.x == 0) {
+        gacc[blockIdx.x] += a.wt * se;
+        gacc[gridDim.x + blockIdx.x] += a.wt * ss;
+    }
+}
+
+// loss pieces at x_T: MSD sum over locals, dU/dsigma sum, and the initial adjoint
+// a_x = (2/N)(x_T + img L - x_0) - F/N, a_v = dt a_x (drift of step T-1)
+__global__ void __launch_bounds__(kT)
+k_adj_init(const double4* __restrict__ pos, const int* __restrict__ img, const int* __restrict__ ref,
+           const double4* __restrict__ x0, const double4* __restrict__ frc, const float4* __restrict__ frc32,
+           int mixed, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, double4* __restrict__ ax,
+           double4* __restrict__ av, double* __restrict__ part, int N, int stride, int nbcap, double rc2,
+           double sigma6, double eps, double inv_sigma, double len0, double len1, double len2, double dt) {
+    __shared__ double scratch[kT / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double msd = 0.0, dus = 0.0;
+    if (i < N) {
+        const double4 p = pos[i];
+        const int im = img[i];
+        const double4 o = x0[ref[i]];
+        const double ux = p.x + len0 * wrap_diff(unpack_axis(im, 0), 0) - o.x;
+        const double uy = p.y + len1 * wrap_diff(unpack_axis(im, 1), 0) - o.y;
+        const double uz = p.z + len2 * wrap_diff(unpack_axis(im, 2), 0) - o.z;
+        msd = ux * ux + uy * uy + uz * uz;
+        double fx, fy, fz;
+        if (mixed) {
+            fx = frc32[i].x; fy = frc32[i].y; fz = frc32[i].z;
+        } else {
+            fx = frc[i].x; fy = frc[i].y; fz = frc[i].z;
+        }
+        const double inv_n = 1.0 / N;
+        const double4 a = make_double4(2.0 * inv_n * ux - fx * inv_n, 2.0 * inv_n * uy - fy * inv_n,
+                                       2.0 * inv_n * uz - fz * inv_n, 0.0);
+        ax[i] = a;
+        av[i] = make_double4(dt * a.x, dt * a.y, dt * a.z, 0.0);
+        const int n = min(nbn[i], nbcap);
+        for (int k = 0; k < n; ++k) {
+            const int j = (int)(__ldg(nbl + (size_t)k * stride + i) >> kCodeBits);
+            const double4 q = pos[j];
+            const double dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+            const double s = dx * dx + dy * dy + dz * dz;
+            if (s < rc2) {
+                const double sr2 = 1.0 / s;
+                const double sr6 = sr2 * sr2 * sr2 * sigma6;
+                dus += 12.0 * eps * inv_sigma * (2.0 * sr6 * sr6 - sr6);  // full list: 1/2 of 24 eps/sigma (...)
+            }
+        }
+    }
+    const double a1 = block_sum(msd, scratch);
+    const double a2 = block_sum(dus, scratch);
+    if (threadIdx.x == 0) {
+        part[blockIdx.x] = a1;
+        part[gridDim.x + blockIdx.x] = a2;
+    }
+}
+
+__global__ void k_sum_rows(const double* __restrict__ part, double* __restrict__ out, int nb, int rows) {
+    __shared__ double scratch[32];
+    for (int q = 0; q < rows; ++q) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) v += part[q * nb + b];
+        const double r = block_sum(v, scratch);
+        if (threadIdx.x == 0) out[q] = r;
+    }
+}
+
+// slot order -> reference order (locals)
+__global__ void k_to_ref(const double4* __restrict__ src, const int* __restrict__ ref, double4* __restrict__ dst,
+                         int N) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < N) dst[ref[s]] = src[s];
+}
+// reference order -> slot order (locals)
+__global__ void k_from_ref(const double4* __restrict__ src, const int* __restrict__ ref, double4* __restrict__ dst,
+                           int N) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < N) dst[s] = src[ref[s]];
+}
+// checkpoint of the current state in reference order
+__global__ void k_checkpoint(const double4* __restrict__ pos, const double4* __restrict__ vel,
+                             const int* __restrict__ img, const int* __restrict__ ref, double4* __restrict__ cx,
+                             double4* __restrict__ cv, int* __restrict__ ci, int N) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < N) {
+        const int r = ref[s];
+        cx[r] = pos[s];
+        cv[r] = vel[s];
+        ci[r] = img[s];
+    }
+}
+// restore a checkpoint into the identity layout (slot = reference index)
+__global__ void k_restore(const double4* __restrict__ cx, const double4* __restrict__ cv,
+                          const int* __restrict__ ci, const double* __restrict__ mass_ref, double4* __restrict__ pos,
+                          double4* __restrict__ vel, int* __restrict__ img, int* __restrict__ ref,
+                          int* __restrict__ slot_of_ref, double* __restrict__ mass, int N) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < N) {
+        pos[r] = cx[r];
+        vel[r] = cv[r];
+        img[r] = ci[r];
+        ref[r] = r;
+        slot_of_ref[r] = r;
+        mass[r] = mass_ref[r];
+    }
+}
+
+double* mass_ref = nullptr;
+
+template <class T>
+void ensure(T** p, int& cap, size_t need) {
+    if ((size_t)cap >= need && *p) return;
+    dfree(p);
+    dalloc(p, need);
+    cap = (int)need;
+}
+
+void free_adjoint() {
+    dfree(&ck_x); dfree(&ck_v); dfree(&ck_img); dfree(&x0_dev); dfree(&seg_x); dfree(&ax);
+    dfree(&av[0]); dfree(&av[1]); dfree(&tmp4); dfree(&gacc); dfree(&red); dfree(&mass_ref);
+    cap_n = cap_seg = cap_ck = 0;
+}
+
+// the list and layout for positions at the start of a segment (already wrapped)
+void rebuild(State& s) {
+    run_borders(s);
+    run_distribute(s);
+    run_build_lists(s, false, cfg.cutoff + cfg.skin);
+}
+
+void reset_identity(State& s, int ckpt) {
+    const int N = s.N;
+    s.G = 0;
+    s.pc = s.vc = s.ac = 0;
+    k_restore<<<nblk(N), kT, 0, s.stream>>>(ck_x + (size_t)ckpt * N, ck_v + (size_t)ckpt * N,
+                                           ck_img + (size_t)ckpt * N, mass_ref, s.pos.b[0], s.vel.b[0], s.img.b[0],
+                                           s.ref.b[0], s.slot_of_ref, s.mass.b[0], N);
+    launched(K_ADJ_STEP);
+}
+
+PendingForce force_params() {
+    PendingForce p;
+    p.valid = true;
+    p.rc = cfg.cutoff;
+    p.eps = run.eps;
+    p.sigma = run.sigma;
+    return p;
+}
+
+void checkpoint(State& s, int k) {
+    const int N = s.N;
+    k_checkpoint<<<nblk(N), kT, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.img.b[s.ac], s.ref.b[s.ac],
+                                              ck_x + (size_t)k * N, ck_v + (size_t)k * N, ck_img + (size_t)k * N, N);
+    launched(K_ADJ_STEP);
+}
+
+// one forward step t (positions x_t -> x_{t+1}); reneighbours when (t+1) % R == 0
+void forward_step(State& s, int t, bool allow_reneigh) {
+    const bool ren = allow_reneigh && (t + 1) % cfg.reneigh == 0;
+    if (ren) {
+        run_integrate(s, cfg.dt, false);
+        run_enforce_pbc(s);
+        rebuild(s);
+    } else {
+        run_integrate(s, cfg.dt, true);
+    }
+    run_force_lj(s, force_params(), true, cfg.dt);
+}
+
+struct ModeGuard {  // the adjoint runs exact ghosts, full lists, its own precision, no thermo
+    int prec, ghost, thermo, half;
+    explicit ModeGuard(State& s) : prec(s.precision), ghost(s.ghost_exact), thermo(s.thermo), half(s.half_ghost) {
+        s.precision = cfg.precision;
+        s.ghost_exact = 1;
+        s.thermo = 0;
+        s.half_ghost = 0;
+    }
+    void restore(State& s) {
+        s.precision = prec;
+        s.ghost_exact = ghost;
+        s.thermo = thermo;
+        s.half_ghost = half;
+    }
+};
+
+}  // namespace
+}  // namespace tmd
 
 using namespace tmd;
 
 extern "C" {
-int md_adjoint_configure(int, int, double, double, double, int) {
-    set_error(MD_ERR_UNSUPPORTED, "adjoint form not built");
-    return -1;
+
+int md_adjoint_configure(int steps, int reneigh, double dt, double cutoff, double skin, int precision) {
+    if (steps < 1 || reneigh < 1 || !(dt > 0) || !(cutoff > 0) || skin < 0) {
+        set_error(MD_ERR_ARGUMENT, "md_adjoint_configure: invalid arguments");
+        return -1;
+    }
+    cfg.configured = true;
+    cfg.steps = steps;
+    cfg.reneigh = reneigh;
+    cfg.dt = dt;
+    cfg.cutoff = cutoff;
+    cfg.skin = skin;
+    cfg.precision = precision ? 1 : 0;
+    run.forward_done = false;
+    return 0;
 }
-int md_adjoint_forward(double const*, double, double, double*) { return -1; }
-int md_adjoint_backward(double*, double*, double*) { return -1; }
-int md_adjoint_times(double*, double*) { return -1; }
+
+int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* loss) {
+    State& s = g_state;
+    if (!s.alive || !cfg.configured) {
+        set_error(MD_ERR_STATE, "md_adjoint_forward: initialise the grid and call md_adjoint_configure first");
+        return -1;
+    }
+    md_synchronize();
+    const int N = s.N;
+    run.eps = epsilon;
+    run.sigma = sigma;
+    run.nseg = (cfg.steps + cfg.reneigh - 1) / cfg.reneigh;
+    ensure(&ck_x, cap_ck, (size_t)run.nseg * N);
+    {
+        int c1 = 0, c2 = 0;
+        dfree(&ck_v);
+        dfree(&ck_img);
+        dalloc(&ck_v, (size_t)run.nseg * N);
+        dalloc(&ck_img, (size_t)run.nseg * N);
+        (void)c1;
+        (void)c2;
+    }
+    int cap_tmp = 0;
+    dfree(&x0_dev);
+    dalloc(&x0_dev, N);
+    dfree(&mass_ref);
+    dalloc(&mass_ref, N);
+    (void)cap_tmp;
+    // initial state in reference order: x_0 from md_initialize_grid, v_0 from the caller
+    std::vector<double4> hx(N), hv(N);
+    for (int i = 0; i < N; ++i) {
+        hx[i] = make_double4(s.h_x0[3 * i], s.h_x0[3 * i + 1], s.h_x0[3 * i + 2], 0.0);
+        hv[i] = make_double4(v0[3 * i], v0[3 * i + 1], v0[3 * i + 2], 0.0);
+    }
+    std::vector<double> hm(s.h_mass.begin(), s.h_mass.begin() + N);
+    TMD_CUDA(cudaMemcpyAsync(x0_dev, hx.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(ck_x, hx.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(ck_v, hv.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemsetAsync(ck_img, 0, sizeof(int) * N, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(mass_ref, hm.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s.stream));
+    ModeGuard guard(s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s.stream);
+    reset_identity(s, 0);
+    rebuild(s);
+    run_force_lj(s, force_params(), false, 0.0);
+    for (int t = 0; t < cfg.steps; ++t) {
+        if (t + 1 == cfg.steps) s.thermo = 1;  // U(x_T) for the loss
+        forward_step(s, t, true);
+        if ((t + 1) % cfg.reneigh == 0 && t + 1 < cfg.steps) checkpoint(s, (t + 1) / cfg.reneigh);
+    }
+    s.thermo = 0;
+    cudaEventRecord(e1, s.stream);
+    // loss: MSD and U at x_T, and the initial adjoint state
+    const int nb = nblk(N);
+    int capd = 0;
+    dfree(&ax);
+    dalloc(&ax, N);
+    dfree(&av[0]);
+    dfree(&av[1]);
+    dalloc(&av[0], N);
+    dalloc(&av[1], N);
+    dfree(&tmp4);
+    dalloc(&tmp4, N);
+    dfree(&gacc);
+    dalloc(&gacc, 2 * (size_t)nb + 2);
+    dfree(&red);
+    dalloc(&red, 8);
+    (void)capd;
+    ensure_red_scratch(s, 2 * nb);
+    const double sig6 = std::pow(sigma, 6);
+    k_adj_init<<<nb, kT, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.ref.b[s.ac], x0_dev, s.frc.b[s.ac], s.frc32,
+                                       s.precision, s.nbn, s.nbl, ax, av[0], s.red_part, N, s.nb_stride, s.nb_cap,
+                                       cfg.cutoff * cfg.cutoff, sig6, epsilon, 1.0 / sigma, s.geo.len[0],
+                                       s.geo.len[1], s.geo.len[2], cfg.dt);
+    launched(K_ADJ_STEP);
+    k_sum_rows<<<1, 256, 0, s.stream>>>(s.red_part, red, nb, 2);
+    launched(K_ADJ_STEP);
+    double sums[2] = {0, 0}, th[4] = {0, 0, 0, 0};
+    TMD_CUDA(cudaMemcpyAsync(sums, red, sizeof(sums), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(th, s.thermo_dev, sizeof(th), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    float fms = 0.f;
+    cudaEventElapsedTime(&fms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    run.fwd_ms = fms;
+    run.U = 0.5 * th[0];
+    double dUds = sums[1];
+    if (cfg.shifted) {
+        // U_s = U - (pairs inside the cutoff) * e_c, e_c = 4 eps ((sigma/rc)^12 - (sigma/rc)^6);
+        // th[2] counts list entries inside the cutoff (each pair twice)
+        const double pairs = 0.5 * th[2];
+        const double src6 = sig6 / std::pow(cfg.cutoff, 6);
+        const double ec = 4.0 * epsilon * (src6 * src6 - src6);
+        const double dec_ds = 4.0 * epsilon * (12.0 * src6 * src6 - 6.0 * src6) / sigma;
+        run.U -= pairs * ec;
+        dUds -= pairs * dec_ds;
+    }
+    run.loss = sums[0] / N + run.U / N;
+    // the direct theta terms of U(x_T)/N; the reverse pass adds the trajectory terms
+    std::vector<double> g0(2 * (size_t)nb + 2, 0.0);
+    g0[2 * (size_t)nb] = run.U / (N * epsilon);
+    g0[2 * (size_t)nb + 1] = dUds / N;
+    TMD_CUDA(cudaMemcpyAsync(gacc, g0.data(), sizeof(double) * g0.size(), cudaMemcpyHostToDevice, s.stream));
+    // adjoint state to reference order (the backward pass starts in another layout)
+    k_to_ref<<<nb, kT, 0, s.stream>>>(ax, s.ref.b[s.ac], tmp4, N);
+    launched(K_ADJ_STEP);
+    TMD_CUDA(cudaMemcpyAsync(ax, tmp4, sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+    k_to_ref<<<nb, kT, 0, s.stream>>>(av[0], s.ref.b[s.ac], tmp4, N);
+    launched(K_ADJ_STEP);
+    TMD_CUDA(cudaMemcpyAsync(av[0], tmp4, sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    guard.restore(s);
+    *loss = run.loss;
+    run.forward_done = s.last_error != MD_ERR_CUDA;
+    return run.forward_done ? 0 : -1;
 }
+
+int md_adjoint_backward(double* grad_v0, double* grad_eps, double* grad_sigma) {
+    State& s = g_state;
+    if (!run.forward_done) {
+        set_error(MD_ERR_STATE, "md_adjoint_backward: run md_adjoint_forward first");
+        return -1;
+    }
+    const int N = s.N;
+    const int nb = nblk(N);
+    const int R = cfg.reneigh;
+    if (cap_seg < R * N || !seg_x) {
+        dfree(&seg_x);
+        dalloc(&seg_x, (size_t)R * N);
+        cap_seg = R * N;
+    }
+    ModeGuard guard(s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s.stream);
+    const double c = 0.5 * cfg.dt;
+    int wcur = 0;  // av[wcur] holds a_v (reference order between segments)
+    for (int seg = run.nseg - 1; seg >= 0; --seg) {
+        const int t0 = seg * R;
+        const int t1 = std::min(t0 + R, cfg.steps);  // positions x_t0 .. x_{t1-1}
+        reset_identity(s, seg);
+        rebuild(s);
+        run_force_lj(s, force_params(), false, 0.0);
+        TMD_CUDA(cudaMemcpyAsync(seg_x, s.pos.b[s.pc], sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+        for (int t = t0; t + 1 < t1; ++t) {
+            forward_step(s, t, false);
+            TMD_CUDA(cudaMemcpyAsync(seg_x + (size_t)(t + 1 - t0) * N, s.pos.b[s.pc], sizeof(double4) * N,
+                                     cudaMemcpyDeviceToDevice, s.stream));
+        }
+        // adjoint state into this segment's slot order
+        const int* ref = s.ref.b[s.ac];
+        k_from_ref<<<nb, kT, 0, s.stream>>>(ax, ref, tmp4, N);
+        launched(K_ADJ_STEP);
+        TMD_CUDA(cudaMemcpyAsync(ax, tmp4, sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+        k_from_ref<<<nb, kT, 0, s.stream>>>(av[wcur], ref, tmp4, N);
+        launched(K_ADJ_STEP);
+        TMD_CUDA(cudaMemcpyAsync(av[wcur], tmp4, sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+        HvpArgs a;
+        a.N = N;
+        a.stride = s.nb_stride;
+        a.nbcap = s.nb_cap;
+        a.rc2 = cfg.cutoff * cfg.cutoff;
+        a.sigma6 = std::pow(run.sigma, 6);
+        a.eps = run.eps;
+        a.inv_sigma = 1.0 / run.sigma;
+        for (int d = 0; d < 3; ++d) a.len[d] = s.geo.len[d];
+        for (int t = t1 - 1; t >= t0; --t) {
+            a.kick = t > 0 ? cfg.dt : c;
+            a.drift = t > 0 ? cfg.dt : 0.0;
+            a.wt = t > 0 ? cfg.dt : c;
+            prof_begin(K_HVP);
+            k_adj_hvp<<<nb, kT, 0, s.stream>>>(seg_x + (size_t)(t - t0) * N, av[wcur], av[1 - wcur], ax, s.nbn,
+                                              s.nbl, s.groot, s.gcode, gacc, a);
+            launched(K_HVP);
+            prof_end(K_HVP);
+            wcur = 1 - wcur;
+        }
+        k_to_ref<<<nb, kT, 0, s.stream>>>(ax, ref, tmp4, N);
+        launched(K_ADJ_STEP);
+        TMD_CUDA(cudaMemcpyAsync(ax, tmp4, sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+        k_to_ref<<<nb, kT, 0, s.stream>>>(av[wcur], ref, tmp4, N);
+        launched(K_ADJ_STEP);
+        TMD_CUDA(cudaMemcpyAsync(av[wcur], tmp4, sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+    }
+    cudaEventRecord(e1, s.stream);
+    // theta gradients: per-block sums plus the direct terms stored after them
+    k_sum_rows<<<1, 256, 0, s.stream>>>(gacc, red, nb, 2);
+    launched(K_ADJ_STEP);
+    double gsum[2] = {0, 0}, direct[2] = {0, 0};
+    std::vector<double4> hv(N);
+    TMD_CUDA(cudaMemcpyAsync(gsum, red, sizeof(gsum), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(direct, gacc + 2 * (size_t)nb, sizeof(direct), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(hv.data(), av[wcur], sizeof(double4) * N, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    float bms = 0.f;
+    cudaEventElapsedTime(&bms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    run.bwd_ms = bms;
+    for (int i = 0; i < N; ++i) {
+        grad_v0[3 * i] = hv[i].x;
+        grad_v0[3 * i + 1] = hv[i].y;
+        grad_v0[3 * i + 2] = hv[i].z;
+    }
+    *grad_eps = gsum[0] + direct[0];
+    *grad_sigma = gsum[1] + direct[1];
+    guard.restore(s);
+    run.forward_done = false;  // the reverse pass consumed the adjoint state
+    return s.last_error == MD_ERR_CUDA ? -1 : 0;
+}
+
+int md_adjoint_set_loss(int shifted_energy) {
+    cfg.shifted = shifted_energy ? 1 : 0;
+    run.forward_done = false;
+    return 0;
+}
+
+int md_adjoint_times(double* forward_ms, double* backward_ms) {
+    *forward_ms = run.fwd_ms;
+    *backward_ms = run.bwd_ms;
+    return 0;
+}
+
+}  // extern "C"

@@ -98,6 +98,7 @@ _EXTENSION_API = {
     "md_adjoint_forward": (_c_int, [_vp, _c_double, _c_double, _vp]),
     "md_adjoint_backward": (_c_int, [_vp, _vp, _vp]),
     "md_adjoint_times": (_c_int, [_vp, _vp]),
+    "md_adjoint_set_loss": (_c_int, [_c_int]),
 }
 
 _ORACLE_API = {

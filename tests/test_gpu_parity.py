@@ -76,6 +76,42 @@ def test_trajectory_bitwise_fp64_full(product, oracle):
         close_all(p, o)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_thermo_sums_match_oracle(product, oracle, precision):
+    """md_get_thermo = {U sum, virial sum, pairs inside the cutoff, v.v} against the oracle's
+    energy, virial and temperature at step 0 and after 20 and 40 steps (driver loop and native
+    loop).  The device reductions sum in another order, so FP64 agrees to 1e-12 relative; the
+    mixed form's pair energies carry its FP32 force error."""
+    product.md_set_precision(precision)
+    product.md_set_thermo(1)
+    p, o = both(product, oracle, cells=(8, 8, 8))
+    tol = 1e-12 if precision == 0 else 1e-5
+    try:
+        n = p.n
+        t, to = np.zeros(4), np.zeros(2)
+        for stage in range(3):
+            if stage == 0:
+                p.force()
+                product.md_final_integration(0.0)
+            elif stage == 1:
+                p.step(0.005, 20)
+                o.step(0.005, 20)
+            else:
+                p.run(0.005, 20)
+                o.step(0.005, 20)
+            assert product.md_get_thermo(tinymd.ptr(t)) == 0
+            oracle.oracle_last_thermo(tinymd.ptr(to))
+            temp = oracle.oracle_temperature()
+            assert t[0] == pytest.approx(to[0], rel=tol), stage
+            assert t[1] == pytest.approx(to[1], rel=tol * 10), stage
+            assert t[3] / (3.0 * n - 3.0) == pytest.approx(temp, rel=1e-12 if precision == 0 else 1e-6), stage
+            assert t[2] == float(round(t[2])) and t[2] > 0
+    finally:
+        close_all(p, o)
+        product.md_set_thermo(0)
+        product.md_set_precision(0)
+
+
 def test_trajectory_exact_ghosts(product, oracle):
     product.md_set_ghost_mode(1)
     oracle.oracle_set_ghost_mode(1)
