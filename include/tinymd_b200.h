@@ -159,6 +159,21 @@ void md_set_ghost_mode(int exact);
  * pairs are kept when the ghost's root local precedes i, and the reaction
  * force goes to that root. */
 void md_set_half_mode(int ghost_pairs);
+/* Tiled full lists (default 0): full-list builds run one block per row
+ * segment of cells and also write per-warp streams of 16-bit halo indices
+ * that the mixed form's force kernel walks against shared-memory staged
+ * positions.  The lists are the same entry for entry; the staged kernel's
+ * forces differ from the plain-list kernel's by FP32 summation order only.
+ * On B200 this path is measured slower than the default per-cell builder and
+ * plain-list kernel, so it is opt-in. */
+void md_set_tile_mode(int enable);
+/* 1 when the current full lists were built by the tiled builder (the mixed
+ * form's force then runs the staged kernel), else 0. */
+int md_tiles_active(void);
+/* out[6] = {tiled lists active, builder halo capacity, largest staged halo of the
+ * current lists, list capacity, blocks the last tiled build could not take,
+ * largest halo seen by the last tiled build}. */
+void md_tile_info(int *out);
 /* DEM contact model: 0 = the reference closure (its contact branch is
  * unreachable, so the force is zero; default), 1 = contact-fixed
  * spring-dashpot with contact radius `radius` (overlap 2R - r > 0). */

@@ -213,12 +213,16 @@ void free_all(State& s) {
     }
     int** ip[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.cnt, &s.cstart, &s.bin_cell,
                   &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.bcount, &s.bsrc_ref, &s.broot_ref, &s.bcode,
-                  &s.nbn, &s.scan_part};
+                  &s.nbn, &s.scan_part, &s.slot_cell, &s.tile_desc, &s.tile_rows};
     for (int** q : ip) dfree(q);
     dfree(&s.frc32);
     dfree(&s.pos32);
     dfree(&s.bmask);
     dfree(&s.nbl);
+    dfree(&s.tile_stream);
+    s.tile_stream_len = 0;
+    s.tiles_valid = 0;
+    s.tile_desc_blocks = 0;
     dfree(&s.red_part);
     dfree(&s.thermo_dev);
     dfree(&s.status_dev);
@@ -247,7 +251,7 @@ void grow_atoms(State& s, int need) {
     int** keep[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.bsrc_ref, &s.broot_ref,
                     &s.bcode};
     for (int** q : keep) realloc_keep(q, o, n, s.stream);
-    int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.nbn};
+    int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.nbn, &s.slot_cell};
     for (int** q : scratch) {
         dfree(q);
         dalloc(q, n);
@@ -261,6 +265,7 @@ void grow_lists(State& s, int rows) {
     s.nb_cap = rows;
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
     s.lists_valid = 0;
+    s.tiles_valid = 0;
 }
 
 namespace {
@@ -277,6 +282,7 @@ void allocate_state(State& s, int N, int nb_cap) {
     dalloc(&s.bcount, (size_t)2 * 26 * nblk + 1);
     s.nb_stride = ((std::max(N, 1) + 31) / 32) * 32;
     s.nb_cap = nb_cap > 0 ? nb_cap : 100;
+    s.tile_cap = 2560;  // tiled-builder halo capacity, grown per grid as halos need
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
     dalloc(&s.thermo_dev, 8);
     dalloc(&s.status_dev, 1);
@@ -910,6 +916,27 @@ void md_set_precision(int mode) {
         if (mode == 1) run_refresh_pos32(s);
     }
     s.precision = mode;
+}
+void md_set_tile_mode(int enable) {
+    if (g_state.alive) flush_all(g_state);
+    g_state.tile_mode = enable ? 1 : 0;
+    g_state.lists_valid = 0;
+    g_state.tiles_valid = 0;
+}
+void md_tile_info(int* out) {
+    State& s = g_state;
+    if (s.alive) flush_all(s);
+    out[0] = s.tiles_valid;
+    out[1] = s.tile_cap;
+    out[2] = s.tile_halo_max;
+    out[3] = s.nb_cap;
+    out[4] = s.status_host ? s.status_host->tile_overflow : 0;
+    out[5] = s.status_host ? s.status_host->halo_max : 0;
+}
+int md_tiles_active(void) {
+    if (!g_state.alive) return 0;
+    flush_all(g_state);
+    return g_state.tiles_valid;
 }
 void md_set_half_mode(int ghost_pairs) {
     if (g_state.alive) flush_all(g_state);

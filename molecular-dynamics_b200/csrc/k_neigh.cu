@@ -288,11 +288,12 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
                           const double* __restrict__ mass_o, double* __restrict__ mass_n,
                           const int* __restrict__ ref_o, int* __restrict__ ref_n, const int* __restrict__ img_o,
                           int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rref,
-                          int* __restrict__ rbk,
+                          int* __restrict__ rbk, const int* __restrict__ bin_cell, int* __restrict__ slot_cell,
                           float4* __restrict__ pos32, int NA, int N, GeoArgs a, int mixed) {
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= NA) return;
     int o = perm[n];
+    slot_cell[n] = bin_cell[o];
     double4 p = pos_o[o];
     pos_n[n] = p;
     vel_n[n] = vel_o[o];
@@ -620,6 +621,7 @@ void run_borders(State& s) {
     prof_end(K_BORDER);
     s.G = G;
     s.lists_valid = 0;
+    s.tiles_valid = 0;
 }
 
 void run_distribute(State& s) {
@@ -643,7 +645,7 @@ void run_distribute(State& s) {
     const int np = 1 - s.pc, nv = 1 - s.vc, na = 1 - s.ac;
     k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
         s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
-        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk, s.pos32, NA, N, a,
+        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk, s.bin_cell, s.slot_cell, s.pos32, NA, N, a,
         s.precision);
     launched(K_BIN);
     s.pc = np;
@@ -656,6 +658,7 @@ void run_distribute(State& s) {
     }
     prof_end(K_BIN);
     s.lists_valid = 0;
+    s.tiles_valid = 0;
 }
 
 void grow_lists(State& s, int rows);  // api.cu
@@ -667,6 +670,11 @@ int run_build_lists(State& s, bool half, double cutoff) {
         s.lists_half = half;
         return 0;
     }
+    // full lists come from the tiled builder where the grid allows (it also
+    // writes the plain list); a tile whose halo exceeds the staging capacity
+    // sends the whole build back to k_build_list
+    bool use_tiles = !half && tiles_usable(s);
+    s.tiles_valid = 0;
     for (int attempt = 0; attempt < 8; ++attempt) {
         NlArgs a;
         a.cut2 = cutoff * cutoff;
@@ -682,22 +690,40 @@ int run_build_lists(State& s, bool half, double cutoff) {
         for (int d = 0; d < 3; ++d) a.alo[d] = g.aabb_lo[d];
         a.spacing = g.spacing;
         TMD_CUDA(cudaMemsetAsync(&s.status_dev->max_nb, 0, sizeof(int), s.stream));
-        TMD_CUDA(cudaMemsetAsync(&s.status_dev->bad_code, 0, sizeof(int), s.stream));
+        // bad_code, tile_overflow, halo_max and tile_blocks are adjacent
+        TMD_CUDA(cudaMemsetAsync(&s.status_dev->bad_code, 0, 4 * sizeof(int), s.stream));
         prof_begin(K_NLIST);
         const int nb = nblocks(g.ncells, kNlWarps);
-        if (half && s.half_ghost)
-            k_build_list<2><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart,
-                                                                s.nbn, s.nbl, s.status_dev, a);
-        else if (half)
-            k_build_list<1><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                s.nbn, s.nbl, s.status_dev, a);
-        else
-            k_build_list<0><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                s.nbn, s.nbl, s.status_dev, a);
+        // the tiled builder declines when its shared-memory need (halo capacity and
+        // list capacity, both of which grow between attempts) exceeds the limit
+        if (use_tiles && run_build_tiles(s, cutoff) != 1) use_tiles = false;
+        if (!use_tiles) {
+            if (half && s.half_ghost)
+                k_build_list<2><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart,
+                                                                    s.nbn, s.nbl, s.status_dev, a);
+            else if (half)
+                k_build_list<1><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                    s.nbn, s.nbl, s.status_dev, a);
+            else
+                k_build_list<0><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                    s.nbn, s.nbl, s.status_dev, a);
+        }
         launched(K_NLIST);
         prof_end(K_NLIST);
         TMD_CUDA(cudaMemcpyAsync(s.status_host, s.status_dev, sizeof(DevStatus), cudaMemcpyDeviceToHost, s.stream));
         TMD_CUDA(cudaStreamSynchronize(s.stream));
+        if (use_tiles && s.status_host->tile_overflow > 0) {
+            use_tiles = false;  // rows or rebasing cells the tiles cannot take
+            --attempt;
+            continue;
+        }
+        if (use_tiles && s.status_host->halo_max > s.tile_cap) {
+            const int cap = (s.status_host->halo_max + 255) / 256 * 256;
+            if (tile_cap_fits(s, cap)) s.tile_cap = cap;
+            else use_tiles = false;
+            --attempt;
+            continue;
+        }
         if (s.status_host->out_local > 0) {
             int first_out = 0;
             // locals outside the grid sit at [cstart[ncells], N)
@@ -713,6 +739,9 @@ int run_build_lists(State& s, bool half, double cutoff) {
         if (mx <= s.nb_cap) {
             s.lists_valid = 1;
             s.lists_half = half;
+            s.tiles_valid = use_tiles ? 1 : 0;
+            s.tile_halo_max = use_tiles ? s.status_host->halo_max : 0;
+            s.tile_blocks = use_tiles ? s.status_host->tile_blocks : 0;
             return 0;
         }
         // core/neighborlist.impala:74-76: grow to twice the overflow and redo

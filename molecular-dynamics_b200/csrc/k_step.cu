@@ -13,6 +13,7 @@
 // warp one coalesced 128-byte line per neighbour slot, and neighbour
 // positions come through the read-only path.
 
+#include "lj_args.cuh"
 #include "md_common.cuh"
 #include "md_state.h"
 
@@ -29,14 +30,6 @@ struct StepArgs {
     int N, G, stride;
     double dt, h;  // h = 0.5 * dt as the reference computes it
     double len[3], alo[3], rb_h;
-};
-
-struct LjArgs {
-    int N, stride, nbcap;
-    double rc2, sigma6, eps, h;
-    // mixed form
-    float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f;
-    float hx, hy, hz;  // -rb_h, -rb_h/4, -rb_h/16 (shift decode scales)
 };
 
 struct DemArgs {
@@ -165,6 +158,29 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
 }
 
 // ---- mixed LJ -----------------------------------------------------------------
+// FP64 evaluation of one list pair (the mixed form's fallback for close pairs
+// and pairs at the cutoff): accumulates the force on i into c and the thermo sums
+template <bool THERMO>
+__device__ __forceinline__ void fp64_lj(const double4& pi, int j, const double4* __restrict__ pos, const LjArgs& a,
+                                        double& cx, double& cy, double& cz, double& e, double& w, int& ncnt) {
+    const double4 pj = ldg_d4(pos + j);
+    const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
+    const double r2 = len2_strict(ex, ey, ez);
+    if (r2 < a.rc2) {
+        const double sr2 = 1.0 / r2;
+        const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
+        const double f = 48.0 * sr6 * (sr6 - 0.5) * sr2 * a.eps;
+        cx += ex * f;
+        cy += ey * f;
+        cz += ez * f;
+        if (THERMO) {
+            e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
+            w += f * r2;
+            ncnt++;
+        }
+    }
+}
+
 // FP32 pair arithmetic on positions rebased to a dyadic grid of spacing rb_h:
 // del = (r_i - r_j) - dk*rb_h, with dk in {-1,0,1}^3 decoded from the list
 // entry's low bits (exact float construction, 3 operations per axis) and the
@@ -188,6 +204,7 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
+        int nq = 0, q0 = 0, q1 = 0;  // deferred FP64 pairs
         const uint32_t* lp = nbl + i;
         for (int k0 = 0; k0 < n; k0 += kB32) {
             uint32_t ent[kB32];
@@ -229,7 +246,7 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                         wf += f * rsq;
                         ncnt++;
                     }
-                } else {
+                } else if (HALF) {
                     // FP64 path: exact cutoff decision and close-contact accuracy
                     const double4 pj = ldg_d4(pos + j);
                     const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
@@ -241,20 +258,35 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                         cx += ex * f;
                         cy += ey * f;
                         cz += ez * f;
-                        if (HALF) {
-                            const int t = reaction_slot(j, a.N, groot);
-                            atomicAdd(&frc32[t].x, (float)(-ex * f));
-                            atomicAdd(&frc32[t].y, (float)(-ey * f));
-                            atomicAdd(&frc32[t].z, (float)(-ez * f));
-                        }
+                        const int t = reaction_slot(j, a.N, groot);
+                        atomicAdd(&frc32[t].x, (float)(-ex * f));
+                        atomicAdd(&frc32[t].y, (float)(-ey * f));
+                        atomicAdd(&frc32[t].z, (float)(-ez * f));
                         if (THERMO) {
                             e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
                             w += f * r2;
                             ncnt++;
                         }
                     }
+                } else {
+                    // FP64 path, deferred: the pair joins a short queue that is worked off in
+                    // list order after the loop (or when full), so a warp's rare FP64 pairs run
+                    // together instead of each stalling the warp; the FP64 sum sees the same
+                    // terms in the same order
+                    if (nq == 2) {
+                        fp64_lj<THERMO>(pi, q0, pos, a, cx, cy, cz, e, w, ncnt);
+                        fp64_lj<THERMO>(pi, q1, pos, a, cx, cy, cz, e, w, ncnt);
+                        nq = 0;
+                    }
+                    if (nq == 0) q0 = j;
+                    else q1 = j;
+                    ++nq;
                 }
             }
+        }
+        if (!HALF) {
+            if (nq > 0) fp64_lj<THERMO>(pi, q0, pos, a, cx, cy, cz, e, w, ncnt);
+            if (nq > 1) fp64_lj<THERMO>(pi, q1, pos, a, cx, cy, cz, e, w, ncnt);
         }
         const double Fx = (double)fx + cx, Fy = (double)fy + cy, Fz = (double)fz + cz;
         if (HALF) {
@@ -539,15 +571,6 @@ StepArgs step_args(const State& s, double dt) {
     return a;
 }
 
-double ipow(double x, int n) {  // utils/utilities.impala:27-36
-    if (n == 1) return x;
-    if (n % 2 == 0) {
-        double y = ipow(x, n / 2);
-        return y * y;
-    }
-    return x * ipow(x, n - 1);
-}
-
 template <bool HALF, bool FUSE, bool THERMO>
 void launch_lj(State& s, const LjArgs& a, int nb) {
     double4* vel = s.vel.b[s.vc];
@@ -575,26 +598,20 @@ void run_reduce_thermo(State& s, int nb, int nq) {
     launched(K_REDUCE);
 }
 
+void run_reduce_partials(State& s, int nb, int q0, int q1) {
+    k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, q0, q1);
+    launched(K_REDUCE);
+}
+
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
     const int N = s.N;
     if (N == 0) return;
-    LjArgs a;
-    a.N = N;
-    a.stride = s.nb_stride;
-    a.nbcap = s.nb_cap;
-    a.rc2 = p.rc * p.rc;
-    a.sigma6 = ipow(p.sigma, 6);
-    a.eps = p.eps;
-    a.h = 0.5 * dt;
-    // FP32 rsq of a list pair is within ~4e-6 of the FP64 value (del components
-    // carry at most ~3.6e-7 error); pairs inside this window take the FP64 test
-    const double margin = 2e-5 * a.rc2 + 1e-7;
-    a.rc2_lo = (float)(a.rc2 - margin);
-    a.rc2_hi = (float)(a.rc2 + margin);
-    a.close2 = (float)(p.sigma * p.sigma);
-    a.sig6f = (float)a.sigma6;
-    a.eps48f = (float)(48.0 * p.eps);
-    a.eps4f = (float)(4.0 * p.eps);
+    if (s.precision == 1 && !p.half && s.tiles_valid && !s.lists_half) {
+        run_force_lj_tiles(s, p, fuse_final, dt);
+        return;
+    }
+    LjArgs a = lj_args(s, p, dt);
+    // the list entry's code holds dk + 1 in bits 0-1 (x), 2-3 (y), 4-5 (z)
     a.hx = (float)(-s.geo.rb_h);
     a.hy = (float)(-s.geo.rb_h / 4.0);
     a.hz = (float)(-s.geo.rb_h / 16.0);

@@ -1,0 +1,51 @@
+// lj_args.cuh -- parameters of the LJ force kernels (core/runtime.impala:188-201),
+// shared by the plain-list kernels (k_step.cu) and the tiled kernels (k_tile.cu)
+// so both evaluate a pair with the same constants.
+#pragma once
+
+#include "md_state.h"
+
+namespace tmd {
+
+struct LjArgs {
+    int N, stride, nbcap;
+    double rc2, sigma6, eps, h;
+    // mixed form
+    float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f;
+    float hx, hy, hz;  // shift decode scales (see the kernels)
+};
+
+// utils/utilities.impala:27-36 (recursive squaring) for integer powers
+inline double ipow(double x, int n) {
+    if (n == 1) return x;
+    if (n % 2 == 0) {
+        double y = ipow(x, n / 2);
+        return y * y;
+    }
+    return x * ipow(x, n - 1);
+}
+
+// hx, hy, hz are left to the caller (they depend on how the kernel packs dk)
+inline LjArgs lj_args(const State& s, const PendingForce& p, double dt) {
+    LjArgs a;
+    a.N = s.N;
+    a.stride = s.nb_stride;
+    a.nbcap = s.nb_cap;
+    a.rc2 = p.rc * p.rc;
+    a.sigma6 = ipow(p.sigma, 6);
+    a.eps = p.eps;
+    a.h = 0.5 * dt;
+    // FP32 rsq of a list pair is within ~4e-6 of the FP64 value (del components
+    // carry at most ~3.6e-7 error); pairs inside this window take the FP64 test
+    const double margin = 2e-5 * a.rc2 + 1e-7;
+    a.rc2_lo = (float)(a.rc2 - margin);
+    a.rc2_hi = (float)(a.rc2 + margin);
+    a.close2 = (float)(p.sigma * p.sigma);
+    a.sig6f = (float)a.sigma6;
+    a.eps48f = (float)(48.0 * p.eps);
+    a.eps4f = (float)(4.0 * p.eps);
+    a.hx = a.hy = a.hz = 0.0f;
+    return a;
+}
+
+}  // namespace tmd

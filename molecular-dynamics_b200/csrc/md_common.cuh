@@ -35,13 +35,14 @@ __device__ __forceinline__ int unpack_axis(int p, int axis) { return (p >> (10 *
 __device__ __forceinline__ int wrap_diff(int a, int b) { return ((a - b + 512) & 1023) - 512; }
 
 // FP32 copy of a position relative to the centre of its cell in the dyadic
-// rebasing grid of spacing h (mixed form)
+// rebasing grid of spacing h (mixed form); w carries the packed rebasing cell
+// (bit pattern of rbk), which the staged force kernel decodes
 __device__ __forceinline__ float4 rebased32(const double4& p, int rbk, const double* alo, double h) {
     float4 r;
     r.x = (float)(p.x - (alo[0] + ((double)unpack_axis(rbk, 0) + 0.5) * h));
     r.y = (float)(p.y - (alo[1] + ((double)unpack_axis(rbk, 1) + 0.5) * h));
     r.z = (float)(p.z - (alo[2] + ((double)unpack_axis(rbk, 2) + 0.5) * h));
-    r.w = 0.0f;
+    r.w = __int_as_float(rbk);
     return r;
 }
 

@@ -54,7 +54,9 @@ struct DevStatus {
     int out_local;      // locals outside the cell grid at the last binning
     int out_ghost;      // ghosts outside the cell grid
     int bad_code;       // list pairs whose rebasing offset exceeded one cell
-    int pad[3];
+    int tile_overflow;  // slot blocks the tiled builder could not take (halo or row limits)
+    int halo_max;       // largest staged halo of the last tiled build
+    int tile_blocks;    // row blocks of the last tiled build
 };
 
 struct PendingForce {
@@ -110,6 +112,7 @@ struct State {
     int* tmp_key = nullptr;    // per sorted position: reference index
     int* tmp_src = nullptr;    // per sorted position: old slot
     int* perm = nullptr;       // new slot -> old slot
+    int* slot_cell = nullptr;  // per (sorted) slot: its cell, ncells when outside the grid
     // border pass
     unsigned* bmask = nullptr;   // per local (reference order): 26-bit ghost-type mask
     int* bcount = nullptr;       // [26][nblk] counts, scanned in place
@@ -119,6 +122,18 @@ struct State {
     // neighbour lists
     int* nbn = nullptr;
     uint32_t* nbl = nullptr;
+    // tiled full lists (k_tile.cu): per warp of a row block, its homes' lists of
+    // halo indices into the block's staged candidates, concatenated home-major
+    uint16_t* tile_stream = nullptr;
+    size_t tile_stream_len = 0;
+    int tile_mode = 0;       // build and use tiled full lists where the grid allows (opt-in)
+    int tiles_valid = 0;     // tile_stream matches the current cells
+    int tile_halo_max = 0;   // largest halo of the current tiled lists (staged atoms)
+    int tile_cap = 2560;     // halo capacity of the tiled builder (grows to fit)
+    int* tile_desc = nullptr;  // per row block: homes, runs and halo ranges (k_tile.cu)
+    int* tile_rows = nullptr;  // per row of cells: blocks, then their exclusive scan
+    int tile_desc_blocks = 0;  // descriptor capacity (blocks)
+    int tile_blocks = 0;       // row blocks of the current tiled lists
     // scan scratch, reductions, status
     int* scan_part = nullptr;  int scan_part_cap = 0;
     double* red_part = nullptr; int red_part_cap = 0;
@@ -171,6 +186,12 @@ void run_enforce_pbc(State& s);
 void run_borders(State& s);                       // ghost generation, reference order
 void run_distribute(State& s);                    // binning + reorder
 int run_build_lists(State& s, bool half, double cutoff);  // returns 0 or error
+// tiled full-list build (k_tile.cu): 1 = built, 0 = not applicable (caller builds
+// the plain list), -1 = error
+int run_build_tiles(State& s, double cutoff);
+bool tiles_usable(const State& s);
+bool tile_cap_fits(const State& s, int cap);  // the tiled builder can stage halos of `cap` atoms
+void run_force_lj_tiles(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_dem(State& s, const PendingForce& p);
 void run_integrate(State& s, double dt, bool fuse_ghosts);
@@ -178,6 +199,8 @@ void run_ghost_sync(State& s);
 void run_final(State& s, double dt);
 void run_refresh_pos32(State& s);
 void run_reduce_thermo(State& s, int nblocks, int nq);
+// sums the [q][nblocks] per-block partials of quantities q0..q1-1 into thermo_dev[q]
+void run_reduce_partials(State& s, int nblocks, int q0, int q1);
 void exclusive_scan(State& s, const int* in, int* out, int n);
 void ensure_scan_scratch(State& s, int n);
 void ensure_red_scratch(State& s, int n);
