@@ -325,6 +325,15 @@ __global__ void k_ghost_links(const int* __restrict__ ref, const int* __restrict
 }
 
 // ---- neighbour lists ---------------------------------------------------------
+// rebasing cell k relative to b, 8 bits per axis with bias 128 (|k - b| < 128 per axis
+// for atoms a few cells apart); differences of two such values carry no borrow while
+// every axis differs by at most 1
+__device__ __forceinline__ int rel_cell(int k, int b) {
+    return (wrap_diff(unpack_axis(k, 0), unpack_axis(b, 0)) + 128) |
+           ((wrap_diff(unpack_axis(k, 1), unpack_axis(b, 1)) + 128) << 8) |
+           ((wrap_diff(unpack_axis(k, 2), unpack_axis(b, 2)) + 128) << 16);
+}
+
 constexpr int kNlWarps = 4;    // warps (cells) per block
 constexpr int kTile = 128;     // staged candidates per warp and tile
 constexpr int kHomeMax = 64;   // home atoms handled per pass over the candidates
@@ -392,6 +401,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
     const double ctr[3] = {a.alo[0] + ((double)cx + 0.5) * a.spacing, a.alo[1] + ((double)cy + 0.5) * a.spacing,
                            a.alo[2] + ((double)cz + 0.5) * a.spacing};
     int maxcnt = 0;
+    const int rb0 = __ldg(rbk + h0);  // rebasing cells are staged relative to the first home's
 
     for (int hb = h0; hb < h1; hb += kHomeMax) {
         const int hn = min(kHomeMax, h1 - hb);
@@ -403,23 +413,26 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
         __syncwarp();
         for (int t0 = 0; t0 < M; t0 += kTile) {
             const int tn = min(kTile, M - t0);
-            for (int q = 0; q < 54; ++q) {
-                const int ra = max(s_rpre[wid][q], t0), rb = min(s_rpre[wid][q + 1], t0 + tn);
-                for (int m = ra + lane; m < rb; m += 32) {
-                    const int slot = s_rstart[wid][q] + (m - s_rpre[wid][q]);
-                    double4 p = pos[slot];
-                    s_cpos[wid][m - t0] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]),
-                                                      (float)(p.z - ctr[2]), __int_as_float(slot));
-                    s_cref[wid][m - t0] = HM ? ref[slot] : 0;  // root reference index (ref for locals)
-                    s_crbk[wid][m - t0] = rbk[slot];
+            for (int m = t0 + lane; m < t0 + tn; m += 32) {
+                int lo = 0, hi = 53;  // the range of candidate m: the last one starting at or before m
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_rpre[wid][mid] <= m) lo = mid;
+                    else hi = mid - 1;
                 }
+                const int slot = s_rstart[wid][lo] + (m - s_rpre[wid][lo]);
+                double4 p = pos[slot];
+                s_cpos[wid][m - t0] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]),
+                                                  (float)(p.z - ctr[2]), __int_as_float(slot));
+                s_cref[wid][m - t0] = HM ? ref[slot] : 0;  // root reference index (ref for locals)
+                s_crbk[wid][m - t0] = rel_cell(rbk[slot], rb0);
             }
             __syncwarp();
             for (int h = 0; h < hn; ++h) {
                 const int i = hb + h;
                 const float4 hp = s_hpos[wid][h];
                 const int iref = HM ? ref[i] : 0;
-                const int irbk = rbk[i];
+                const int irel = rel_cell(rbk[i], rb0);
                 int cnt = s_hcnt[wid][h];
                 for (int q0 = 0; q0 < tn; q0 += 32) {
                     const int q = q0 + lane;
@@ -442,15 +455,15 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                         // periodic boundary are kept once
                         pred = in && slot != i && (!HM || s_cref[wid][q] < iref);
                         if (pred) {
-                            const int cr = s_crbk[wid][q];
-                            int dkx = wrap_diff(unpack_axis(cr, 0), unpack_axis(irbk, 0));
-                            int dky = wrap_diff(unpack_axis(cr, 1), unpack_axis(irbk, 1));
-                            int dkz = wrap_diff(unpack_axis(cr, 2), unpack_axis(irbk, 2));
-                            if (dkx < -1 || dkx > 1 || dky < -1 || dky > 1 || dkz < -1 || dkz > 1) {
+                            // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow
+                            // shows up as bits above bit 1 or in byte 3) means |dk| > 1
+                            const uint32_t d = (uint32_t)(s_crbk[wid][q] - irel + 0x010101);
+                            if ((d & 0xFFFCFCFCu) || (d & (d >> 1) & 0x010101u)) {
                                 atomicAdd(&st->bad_code, 1);
-                                dkx = dky = dkz = 0;
+                                code = 21;  // dk = 0
+                            } else {
+                                code = (int)((d & 3u) | ((d >> 6) & 0xCu) | ((d >> 12) & 0x30u));
                             }
-                            code = (dkx + 1) | ((dky + 1) << 2) | ((dkz + 1) << 4);
                         }
                     }
                     const unsigned bal = __ballot_sync(0xffffffffu, pred);

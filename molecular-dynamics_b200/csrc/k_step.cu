@@ -21,7 +21,10 @@ namespace tmd {
 
 namespace {
 
-constexpr int kThreads = 256;
+#ifndef TMD_THREADS
+#define TMD_THREADS 256
+#endif
+constexpr int kThreads = TMD_THREADS;
 constexpr int kThermoQ = 4;  // partials: energy, virial, pairs inside the cutoff, v.v
 
 inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
@@ -79,7 +82,7 @@ __device__ __forceinline__ int reaction_slot(int j, int N, const int* groot) { r
 #define TMD_B32 4
 #endif
 #ifndef TMD_MINB
-#define TMD_MINB 4
+#define TMD_MINB (1024 / TMD_THREADS)  // caps registers at 64 per thread
 #endif
 constexpr int kB64 = TMD_B64;  // neighbours loaded per batch (FP64)
 constexpr int kB32 = TMD_B32;  // neighbours loaded per batch (mixed)
@@ -228,7 +231,8 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                 if (!(rsq < a.rc2_hi)) continue;
                 const int j = (int)(en >> kCodeBits);
                 if (rsq < a.rc2_lo && rsq >= a.close2) {
-                    const float sr2 = __frcp_rn(rsq);
+                    float sr2;  // hardware reciprocal (~1 ulp); the error budget is set by del, not by 1/r^2
+                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
                     const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
                     const float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
                     const float px = dx * f, py = dy * f, pz = dz * f;

@@ -418,7 +418,8 @@ __device__ __forceinline__ void stream_step(int p0, int m, int lane, int warp, i
         const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         if (rsq < a.rc2_hi) {
             if (rsq < a.rc2_lo && rsq >= a.close2) {
-                const float sr2 = __frcp_rn(rsq);
+                float sr2;  // hardware reciprocal, as in k_lj_mixed
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
                 const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
                 const float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
                 fx = dx * f;
