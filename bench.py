@@ -25,6 +25,10 @@ drift   total energy per atom over 1000 steps of the workload, sampled every
 adjoint the differentiable form on 16x16x16 cells (16,384 atoms), 200 steps,
         checkpoints every 20 steps: device time of the backward pass over the
         forward pass.
+workloads the 131k lattice with half lists; the 'half' setup at 64^3 (524,288
+        atoms, lists larger than L2) with its force-kernel roofline; DEM at 48^3
+        (FCC diagonal split and the reference's granular gas, reference closure
+        and contact-fixed model), each in both forms.
 
 --impl reference runs that CPU path alone (all host threads) on the same
 workload and prints the same JSON line.  Under torchrun each rank runs an
@@ -153,6 +157,13 @@ def barrier(dist):
         dist.barrier()
 
 
+def replica_rate(atoms_per_rank, world, steps, ms_local, dist, device=None):
+    """Whole-job atom-steps/s of `world` independent replicas: all ranks' atoms over the
+    slowest rank's time (every rank calls this with its own time, in the same order)."""
+    ms = allreduce_max(ms_local, dist, device)
+    return atoms_per_rank * world * steps / (ms * 1e-3), ms
+
+
 # ---------------------------------------------------------------------------
 def cpu_run(steps, threads, cells=CELLS, warmup=1):
     """The oracle's CPU path on `threads` host threads; returns (atom-steps/s, atoms, seconds)."""
@@ -228,6 +239,72 @@ def energy_drift(lib, tm, parts, precision):
             "end_drift_per_atom": float(e[-1] - e[0])}
 
 
+def measure(lib, tm, parts, precision, steps, warmup, flush, half=False, force_field="lj", dem=(0.0, 0.0, 0.0, 0.0),
+            cutoff=2.5, dt=DT, temp=1.44, profile_force=False):
+    """Device-timed steps of one workload in one form: (atom-steps/s, ms per step, force ms per launch or None)."""
+    lib.md_set_precision(precision)
+    if half:
+        lib.md_set_half_mode(1)  # half lists that keep the periodic-boundary pairs
+    sim = tm.Simulation(lib, *parts, temp=temp, half=half, force_field=force_field, dem=dem, cutoff=cutoff)
+    sim.run(dt, warmup)
+    if profile_force:
+        lib.md_profile_enable(1 << 0)
+        lib.md_profile_reset()
+    step_ms = np.zeros(steps, dtype=np.float32)
+    sim.run(dt, steps, step_ms=step_ms, flush=(ctypes.c_void_p(flush.data_ptr()), flush.numel() * 4))
+    fms = None
+    if profile_force:
+        nl, t = ctypes.c_longlong(), ctypes.c_double()
+        lib.md_profile_get(0, ctypes.byref(nl), ctypes.byref(t))
+        lib.md_profile_enable(0)
+        fms = t.value / max(nl.value, 1)
+    sim.close()
+    lib.md_set_half_mode(0)
+    lib.md_set_precision(0)
+    ms = float(step_ms.astype(np.float64).sum())
+    return len(parts[0]) * steps / (ms * 1e-3), ms / steps, fms
+
+
+def workloads(lib, tm, flush, peak):
+    """The other measured configurations (atom-steps/s in both forms)."""
+    out = {}
+    parts = tm.setup_particles("default", CELLS, lib=lib)
+    row = {"atoms": len(parts[0]), "steps": 300, "lists": "half (periodic-boundary pairs kept, reactions to roots)"}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        row[name] = measure(lib, tm, parts, prec, 300, 20, flush, half=True)[0]
+    row["mixed_over_fp64"] = row["mixed"] / row["fp64"]
+    out["lj_default_fcc_32x32x32_131072_atoms_half_list"] = row
+    # the 'half' setup at 64^3: lists (~160 MB) larger than L2
+    parts = tm.setup_particles("half", (64, 64, 64), lib=lib)
+    row = {"atoms": len(parts[0]), "steps": 500, "lists": "full"}
+    fms = {}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        row[name], _, fms[name] = measure(lib, tm, parts, prec, 500, 20, flush, profile_force=True)
+    row["mixed_over_fp64"] = row["mixed"] / row["fp64"]
+    n = 75.0  # mean full-list length of the FCC liquid at this density (measured at 131k)
+    b32 = 4 + n * (4 + 12) + 12 + 12
+    achieved = len(parts[0]) * b32 / (fms["mixed"] * 1e-3) / 1e9
+    row["roofline_mixed_force"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak, "launch_ms": fms["mixed"], "bytes_per_atom": b32}
+    out["lj_half_fcc_64x64x64_524288_atoms_full_list"] = row
+    # DEM at 48^3: the FCC diagonal split and the reference's granular gas, with the
+    # reference closure (zero force) and the contact-fixed model (R = 0.6)
+    dem = (0.1, 0.1, 100.0, 0.5)  # damping_n, damping_t, stiffness, friction
+    for setup in ("granular_gas_fcc", "granular_gas"):
+        parts = tm.setup_particles(setup, (48, 48, 48), lib=lib)
+        for model, radius in (("reference_closure", 1.0), ("contact_fixed_R0.6", 0.6)):
+            lib.md_set_dem_model(1 if model.startswith("contact") else 0, radius)
+            row = {"atoms": len(parts[0]), "steps": 300, "cutoff": 1.2, "skin": 0.3, "dt": 0.001,
+                   "stiffness": 100.0, "damping_n": 0.1, "damping_t": 0.1, "friction": 0.5}
+            for name, prec in (("fp64", 0), ("mixed", 1)):
+                row[name] = measure(lib, tm, parts, prec, 300, 20, flush, force_field="dem", dem=dem, cutoff=1.2,
+                                    dt=0.001, temp=None)[0]
+            row["mixed_over_fp64"] = row["mixed"] / row["fp64"]
+            out[f"dem_{setup}_48x48x48_{model}"] = row
+    lib.md_set_dem_model(0, 1.0)
+    return out
+
+
 def adjoint_times(lib, tm):
     """Differentiable form on its own workload: 16x16x16 cells (16,384 atoms), 200 steps of dt
     0.005, checkpoints every 20 steps, mixed forward; device ms of one forward and one backward
@@ -273,7 +350,7 @@ def run_ours(args):
     barrier(dist)
     ms64, _ = timed_steps(lib, sim, K, flush)
     sim.close()
-    ms64 = allreduce_max(ms64, dist, dev)
+    value64, ms64 = replica_rate(natoms, world, K, ms64, dist, dev)
 
     # ---- mixed form (headline) ----------------------------------------------------
     lib.md_set_precision(1)
@@ -302,7 +379,7 @@ def run_ours(args):
     _, _, f64 = tm.full_state(lib)
     ferr = float(np.max(np.abs(f32 - f64)) / np.sqrt(np.mean(f64 ** 2)))
     sim.close()
-    ms32 = allreduce_max(ms32, dist, dev)
+    value, ms32 = replica_rate(natoms, world, K, ms32, dist, dev)
 
     drift = {"steps": DRIFT_STEPS, "every": DRIFT_EVERY}
     for name, prec in (("fp64", 0), ("mixed", 1)):
@@ -310,6 +387,7 @@ def run_ours(args):
     drift["mixed_over_fp64"] = drift["mixed"]["max_abs_drift_per_atom"] / max(
         drift["fp64"]["max_abs_drift_per_atom"], 1e-300)
     adj = adjoint_times(lib, tm)
+    more = workloads(lib, tm, flush, peaks()[0])
 
     # ---- end to end through the C ABI with host buffers ---------------------------
     lib.md_set_precision(1)
@@ -325,14 +403,11 @@ def run_ours(args):
         nghost = s.counts()[1]
         s.close()
         e2e_runs.append(t1 - t0)
-    e2e_s = allreduce_max(min(e2e_runs), dist, dev)
+    e2e_value, e2e_ms = replica_rate(natoms, world, K, min(e2e_runs) * 1e3, dist, dev)
     lib.md_set_precision(0)
     h2d = natoms * (8 + 24 + 24)
     d2h = (natoms + nghost) * (32 * 3 + 16 + 8 + 4)  # md_copy_data_from_accelerator
 
-    total_atoms = natoms * world
-    value = total_atoms * K / (ms32 * 1e-3)
-    value64 = total_atoms * K / (ms64 * 1e-3)
     peak, peak_kind = peaks()
     force_ms = fms.value / max(nl.value, 1)
     # algorithmic bytes per atom and force launch (payload only, padding excluded): the list
@@ -353,12 +428,17 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
                      "bytes_per_atom": bytes_per_atom, "mean_list_length": mean_nb,
-                     "launch_ms": force_ms, "launches": nl.value},
-        "e2e": {"value": total_atoms * K / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+                     "launch_ms": force_ms, "launches": nl.value,
+                     # list count and entries plus the atom's own FP64 position and force: what
+                     # must come from HBM once per step whatever the gathers hit
+                     "compulsory_bytes_per_atom": 4 + 4 * mean_nb + 48,
+                     "compulsory_frac": natoms * (4 + 4 * mean_nb + 48) / (force_ms * 1e-3) / 1e9 / peak},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
                 "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock"},
         "drift": drift,
         "adjoint": adj,
+        "workloads": more,
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -368,6 +448,10 @@ def run_ours(args):
         rate, n_cpu, secs = cpu_run(steps, threads)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{n_cpu} atoms x {steps} timesteps of the same workload"}
+        # one thread: what the reference's cpu backend does (its -t flag is only printed)
+        rate1, _, _ = cpu_run(10, 1)
+        line["cpu_baseline_1thread"] = {"value": rate1, "unit": UNIT, "cores": 1, "kind": "port",
+                                        "sample": f"{n_cpu} atoms x 10 timesteps of the same workload"}
     if dist is not None:
         barrier(dist)
         import torch.distributed as td

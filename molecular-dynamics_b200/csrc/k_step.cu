@@ -376,7 +376,9 @@ k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, dou
     if (i >= a.N) return;
     const double4 pi = pos[i];
     const double4 vi = vel[i];
-    const int n = min(nbn[i], a.nbcap);
+    // the reference closure's pair force is exactly zero (r < 2R gives sqrt(r^2) <= 2R, so its
+    // penetration test never passes): the loop would only add +0.0
+    const int n = a.fixed ? min(nbn[i], a.nbcap) : 0;
     double F[3] = {0.0, 0.0, 0.0};
     for (int k = 0; k < n; ++k) {
         const int j = (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits);
@@ -403,6 +405,102 @@ k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, dou
         atomicAdd(&frc[i].z, F[2]);
     } else {
         frc[i] = make_double4(F[0], F[1], F[2], 0.0);
+    }
+}
+
+// Mixed DEM: the contact-fixed model's pair force in FP32 (same expression order
+// as dem_pair) on rebased positions and FP32 relative velocities.  Pairs within a
+// relative 1e-4 of the force cutoff or of the contact distance 2R take dem_pair
+// in FP64, so both decisions are the FP64 ones.  The reference closure's force
+// is zero (its contact branch is unreachable), as in k_dem_fp64.
+struct DemMixedArgs {
+    float rc2_lo, rc2_hi, c2_lo, c2_hi;  // margins around rc^2 and (2R)^2
+    float d2, dn, dt_, k, mu;            // 2R and the model parameters
+    float hx, hy, hz;                    // rebasing shift decode scales (as k_lj_mixed)
+};
+
+template <bool HALF>
+__global__ void __launch_bounds__(kThreads)
+k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, const double4* __restrict__ vel,
+            float4* __restrict__ frc32, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
+            const int* __restrict__ groot, DemArgs a, DemMixedArgs b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.N) return;
+    float fx = 0.f, fy = 0.f, fz = 0.f;
+    double cx = 0.0, cy = 0.0, cz = 0.0;
+    if (a.fixed) {
+        const float4 ri = pos32[i];
+        const double4 vi = vel[i];
+        const float vix = (float)vi.x, viy = (float)vi.y, viz = (float)vi.z;
+        const int n = min(nbn[i], a.nbcap);
+        for (int k = 0; k < n; ++k) {
+            const uint32_t en = __ldg(nbl + (size_t)k * a.stride + i);
+            const int j = (int)(en >> kCodeBits);
+            const float4 rj = __ldg(pos32 + j);
+            const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
+            const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
+            const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
+            const float dx = fmaf(b.hx, sx, ri.x - rj.x);
+            const float dy = fmaf(b.hy, sy, ri.y - rj.y);
+            const float dz = fmaf(b.hz, sz, ri.z - rj.z);
+            const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (!(rsq < b.rc2_hi) || !(rsq < b.c2_hi)) continue;  // beyond the cutoff or no contact
+            if (rsq >= b.rc2_lo || rsq >= b.c2_lo) {
+                // near a decision: the FP64 pair
+                const double4 pi = pos[i], pj = pos[j];
+                const double4 del = make_double4(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z), 0.0);
+                const double r2 = len2_strict(del.x, del.y, del.z);
+                if (r2 < a.rc2) {
+                    double o[3];
+                    dem_pair(del, r2, vi, ldg_d4(vel + j), a, o);
+                    cx += o[0];
+                    cy += o[1];
+                    cz += o[2];
+                    if (HALF) {
+                        const int t = reaction_slot(j, a.N, groot);
+                        atomicAdd(&frc32[t].x, (float)(-o[0]));
+                        atomicAdd(&frc32[t].y, (float)(-o[1]));
+                        atomicAdd(&frc32[t].z, (float)(-o[2]));
+                    }
+                }
+                continue;
+            }
+            const double4 vj = ldg_d4(vel + j);
+            const float len = sqrtf(rsq);
+            if (!(len > 0.f)) continue;
+            const float delta = b.d2 - len;
+            const float inv = 1.0f / len;
+            const float nx = dx * inv, ny = dy * inv, nz = dz * inv;
+            const float rvx = vix - (float)vj.x, rvy = viy - (float)vj.y, rvz = viz - (float)vj.z;
+            const float vn = rvx * nx + rvy * ny + rvz * nz;
+            const float vtx = rvx - nx * vn, vty = rvy - ny * vn, vtz = rvz - nz * vn;
+            const float vtl = sqrtf(vtx * vtx + vty * vty + vtz * vtz);
+            float fn = b.k * delta - b.dn * vn;
+            if (fn < 0.f) fn = 0.f;
+            const float t1 = b.dt_ * vtl, t2 = b.mu * fn;
+            const float ft = t1 < t2 ? t1 : t2;
+            const float tinv = vtl > 0.f ? 1.0f / vtl : 0.f;
+            const float px = nx * fn - vtx * tinv * ft;
+            const float py = ny * fn - vty * tinv * ft;
+            const float pz = nz * fn - vtz * tinv * ft;
+            fx += px;
+            fy += py;
+            fz += pz;
+            if (HALF) {
+                const int t = reaction_slot(j, a.N, groot);
+                atomicAdd(&frc32[t].x, -px);
+                atomicAdd(&frc32[t].y, -py);
+                atomicAdd(&frc32[t].z, -pz);
+            }
+        }
+    }
+    const float Fx = (float)((double)fx + cx), Fy = (float)((double)fy + cy), Fz = (float)((double)fz + cz);
+    if (HALF) {
+        atomicAdd(&frc32[i].x, Fx);
+        atomicAdd(&frc32[i].y, Fy);
+        atomicAdd(&frc32[i].z, Fz);
+    } else {
+        frc32[i] = make_float4(Fx, Fy, Fz, 0.f);
     }
 }
 
@@ -670,6 +768,36 @@ void run_force_dem(State& s, const PendingForce& p) {
     a.k = p.k;
     a.mu = p.mu;
     a.radius = s.dem_radius;
+    if (s.precision == 1) {  // the mixed form's integrators read frc32
+        DemMixedArgs b;
+        const double d2 = 2.0 * (s.dem_fixed ? s.dem_radius : 1.0);
+        b.rc2_lo = (float)(a.rc2 * (1.0 - 1e-4));
+        b.rc2_hi = (float)(a.rc2 * (1.0 + 1e-4));
+        b.c2_lo = (float)(d2 * d2 * (1.0 - 1e-4));
+        b.c2_hi = (float)(d2 * d2 * (1.0 + 1e-4));
+        b.d2 = (float)d2;
+        b.dn = (float)p.dn;
+        b.dt_ = (float)p.dt_;
+        b.k = (float)p.k;
+        b.mu = (float)p.mu;
+        b.hx = (float)(-s.geo.rb_h);
+        b.hy = (float)(-s.geo.rb_h / 4.0);
+        b.hz = (float)(-s.geo.rb_h / 16.0);
+        if (p.half) {
+            k_zero4<<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(nullptr, s.frc32, N);
+            launched(K_MISC);
+        }
+        prof_begin(K_FORCE_DEM);
+        if (p.half)
+            k_dem_mixed<true><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(
+                s.pos32, s.pos.b[s.pc], s.vel.b[s.vc], s.frc32, s.nbn, s.nbl, s.groot, a, b);
+        else
+            k_dem_mixed<false><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(
+                s.pos32, s.pos.b[s.pc], s.vel.b[s.vc], s.frc32, s.nbn, s.nbl, s.groot, a, b);
+        launched(K_FORCE_DEM);
+        prof_end(K_FORCE_DEM);
+        return;
+    }
     if (p.half) {
         k_zero4<<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(s.frc.b[s.ac], nullptr, N);
         launched(K_MISC);
