@@ -371,13 +371,24 @@ def run_ours(args):
     lists = np.zeros((natoms, 1), dtype=np.int32)
     lib.md_get_neighbor_lists(tm.ptr(sizes), tm.ptr(lists), 1)
     mean_nb = float(sizes.mean())
-    # force error of the mixed form on the FP64 form's positions (same state)
+    # force and potential-energy error of the mixed form on the same state: both forms'
+    # forces (and thermo sums) on the positions the timed run ended with
+    lib.md_set_thermo(1)
+    th32, th64 = np.zeros(4), np.zeros(4)
+    sim.force()
+    lib.md_final_integration(0.0)
+    lib.md_get_thermo(tm.ptr(th32))
     _, _, f32 = tm.full_state(lib)
     lib.md_set_precision(0)
     sim.force()
     lib.md_final_integration(0.0)
+    lib.md_get_thermo(tm.ptr(th64))
     _, _, f64 = tm.full_state(lib)
+    lib.md_set_thermo(0)
     ferr = float(np.max(np.abs(f32 - f64)) / np.sqrt(np.mean(f64 ** 2)))
+    u32, u64 = 0.5 * th32[0] / natoms, 0.5 * th64[0] / natoms  # full lists count each pair twice
+    eerr = {"fp64_u_per_atom": u64, "mixed_minus_fp64_u_per_atom": u32 - u64,
+            "relative": abs(u32 - u64) / abs(u64)}
     sim.close()
     value, ms32 = replica_rate(natoms, world, K, ms32, dist, dev)
 
@@ -424,7 +435,7 @@ def run_ours(args):
                    "dt": DT, "reneigh": 20, "cutoff": 2.5, "skin": 0.3, "l2": "flushed before every timed step",
                    "parallelism": f"replicas x{world}"},
         "forms": {"mixed": value, "fp64": value64, "mixed_over_fp64": value / value64,
-                  "mixed_max_force_err_over_rms": ferr},
+                  "mixed_max_force_err_over_rms": ferr, "mixed_energy_err": eerr},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
                      "bytes_per_atom": bytes_per_atom, "mean_list_length": mean_nb,

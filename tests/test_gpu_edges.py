@@ -1,0 +1,63 @@
+"""Edge cases of the timestep on the GPU against the oracle: storage growth and an atom outside
+the cell grid.
+
+The reference grows its capacities on overflow and redoes the step
+(core/grid.impala:183-213, core/neighborlist.impala:74-76); so do the library and the
+oracle.  An atom outside the rank box extended by one cell is in no cell
+(core/grid.impala:302); the library keeps it in an outside bucket, gives it an empty
+list and latches MD_ERR_OUT_OF_GRID (5), a warning.
+"""
+import numpy as np
+import pytest
+
+import tinymd
+from helpers import make_sim
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(product, oracle, steps, **kw):
+    p = make_sim(product, setup_lib=product, **kw)
+    o = make_sim(oracle, setup_lib=product, **kw)
+    try:
+        for chunk in range(steps // 10):
+            p.step(0.005, 10)
+            o.step(0.005, 10)
+            xp, vp, fp = tinymd.full_state(product)
+            xo, vo, fo = tinymd.full_state(oracle)
+            np.testing.assert_array_equal(xp, xo, err_msg=f"positions after {10 * (chunk + 1)} steps")
+            np.testing.assert_array_equal(vp, vo)
+            np.testing.assert_array_equal(fp, fo)
+        lp = tinymd.neighbor_lists(product, p.n)
+        lo = tinymd.neighbor_lists(oracle, o.n)
+        assert all(np.array_equal(a, b) for a, b in zip(lp, lo))
+        return product.md_last_error()
+    finally:
+        p.close()
+        o.close()
+
+
+def test_list_capacity_growth(product, oracle):
+    """List capacity 8 against ~78 neighbours: both grow and redo the build; 40 steps (2 rebuilds)
+    stay bit-identical."""
+    run_both(product, oracle, 40, cells=(6, 6, 6), nb_capacity=8)
+
+
+def test_ghost_capacity_growth(product, oracle):
+    """2x2x2 unit cells: 32 atoms and 633 ghosts, far above the initial slot capacity; 40 steps
+    bit-identical."""
+    run_both(product, oracle, 40, cells=(2, 2, 2))
+
+
+def test_atom_outside_the_grid(product, oracle):
+    """One atom starts 5 length units beyond the upper x face (outside the box extended by one
+    2.8 cell): it is in no cell and no list; its ghost image (shifted by -L) lies inside and is
+    binned; the first rebuild wraps it back.  40 steps bit-identical, and the library latches
+    the out-of-grid warning."""
+    m, x, v, world, rank = tinymd.setup_particles("default", (6, 6, 6), lib=product)
+    x = x.copy()
+    x[0, 0] = world[1] + 5.0
+    product.md_clear_error()
+    code = run_both(product, oracle, 40, particles=(m, x, v, world, rank))
+    assert code == 5
+    product.md_clear_error()
