@@ -210,13 +210,13 @@ void free_all(State& s) {
         dfree(&s.mass.b[b]);
         dfree(&s.ref.b[b]);
         dfree(&s.img.b[b]);
+        dfree(&s.pos32.b[b]);
     }
     int** ip[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.cnt, &s.cstart, &s.bin_cell,
                   &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.bcount, &s.bsrc_ref, &s.broot_ref, &s.bcode,
                   &s.nbn, &s.scan_part, &s.slot_cell, &s.tile_desc, &s.tile_rows};
     for (int** q : ip) dfree(q);
     dfree(&s.frc32);
-    dfree(&s.pos32);
     dfree(&s.bmask);
     dfree(&s.nbl);
     dfree(&s.tile_stream);
@@ -245,9 +245,9 @@ void grow_atoms(State& s, int need) {
         realloc_keep(&s.mass.b[b], o, n, s.stream);
         realloc_keep(&s.ref.b[b], o, n, s.stream);
         realloc_keep(&s.img.b[b], o, n, s.stream);
+        realloc_keep(&s.pos32.b[b], o, n, s.stream);
     }
     realloc_keep(&s.frc32, o, n, s.stream);
-    realloc_keep(&s.pos32, o, n, s.stream);
     int** keep[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.bsrc_ref, &s.broot_ref,
                     &s.bcode};
     for (int** q : keep) realloc_keep(q, o, n, s.stream);
@@ -325,7 +325,26 @@ void flush_force(State& s) {
     launch_force(s, p, false, 0.0);
 }
 
+// a force held back by md_final_integration: launched with its final kick alone
+void flush_final(State& s) {
+    if (!s.pend_final) return;
+    s.pend_final = false;
+    phase_mark(PH_FORCE);
+    launch_force(s, s.final_cfg, true, s.pend_final_dt);
+}
+
+// ghosts after a fused force + initial integration, when no ghost refresh follows: carried
+// over as the unfused initial integration does
+void flush_ghost(State& s) {
+    if (!s.pend_ghost) return;
+    s.pend_ghost = false;
+    phase_mark(PH_FORCE);
+    run_ghost_refresh(s, 0);
+}
+
 void flush_all(State& s) {
+    flush_final(s);
+    flush_ghost(s);
     flush_init(s);
     flush_force(s);
 }
@@ -479,6 +498,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.lists_valid = 0;
     s.pend_init = false;
     s.pend_force = PendingForce();
+    s.pend_final = s.pend_ghost = false;
     s.force_iters = s.rsq_iters = s.integration_iters = 0;
     s.launches = 0;
     allocate_state(s, n, neighborlist_capacity);
@@ -625,6 +645,14 @@ void md_assemble_neighborlists(bool half, double cutoff) {
 void md_initial_integration(double dt) {
     State& s = g_state;
     if (!require_alive("md_initial_integration")) return;
+    if (s.pend_final && !s.pend_ghost && !s.pend_init && !s.pend_force.valid) {
+        // the held-back force, its final kick and this initial integration in one kernel
+        s.pend_final = false;
+        phase_mark(PH_FORCE);
+        run_force_lj_init(s, s.final_cfg, s.pend_final_dt, dt);
+        s.pend_ghost = true;
+        return;
+    }
     flush_all(s);
     s.pend_init = true;
     s.pend_dt = dt;
@@ -633,9 +661,13 @@ void md_initial_integration(double dt) {
 void md_synchronize_ghost_layer(void) {
     State& s = g_state;
     if (!require_alive("md_synchronize_ghost_layer")) return;
+    flush_final(s);
     flush_force(s);
     phase_mark(PH_COMM);
-    if (s.pend_init) {
+    if (s.pend_ghost) {
+        s.pend_ghost = false;
+        run_ghost_refresh(s, s.ghost_exact ? 2 : 1);
+    } else if (s.pend_init) {
         s.pend_init = false;
         run_integrate(s, s.pend_dt, true);
     } else {
@@ -681,11 +713,22 @@ void md_compute_dem(bool half, double rc, double damping_n, double damping_t, do
 void md_final_integration(double dt) {
     State& s = g_state;
     if (!require_alive("md_final_integration")) return;
+    flush_final(s);
+    flush_ghost(s);
     flush_init(s);
     phase_mark(PH_FORCE);
     if (s.pend_force.valid) {
         PendingForce p = s.pend_force;
         s.pend_force.valid = false;
+        if (force_init_fusable(s, p)) {
+            // held back: the next md_initial_integration joins it (one pass over the atoms),
+            // any other call launches it with this kick alone
+            s.pend_final = true;
+            s.pend_final_dt = dt;
+            s.final_cfg = p;
+            s.last_force_half = 0;
+            return;
+        }
         if (!p.dem && !p.half) {
             launch_force(s, p, true, dt);
             return;
@@ -1141,6 +1184,7 @@ int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double 
         if (cfg.dem) md_compute_dem(cfg.half, cfg.rc, cfg.dn, cfg.dt_, cfg.k, cfg.mu);
         else md_compute_lennard_jones(cfg.half, cfg.rc, cfg.eps, cfg.sigma);
         md_final_integration(dt);
+        if (k == steps - 1) flush_all(s);  // the last step's force is inside its time
         if (step_ms) TMD_CUDA(cudaEventRecord(ev[2 * k + 1], s.stream));
     }
     sync_stream(s);

@@ -334,9 +334,15 @@ __device__ __forceinline__ int rel_cell(int k, int b) {
            ((wrap_diff(unpack_axis(k, 2), unpack_axis(b, 2)) + 128) << 16);
 }
 
-constexpr int kNlWarps = 4;    // warps (cells) per block
-constexpr int kTile = 128;     // staged candidates per warp and tile
-constexpr int kHomeMax = 64;   // home atoms handled per pass over the candidates
+#ifndef TMD_NL_WARPS
+#define TMD_NL_WARPS 4
+#endif
+#ifndef TMD_NL_TILE
+#define TMD_NL_TILE 256
+#endif
+constexpr int kNlWarps = TMD_NL_WARPS;  // warps (cells) per block
+constexpr int kTile = TMD_NL_TILE;      // staged candidates per warp and tile
+constexpr int kHomeMax = 64;            // home atoms handled per pass over the candidates
 
 struct NlArgs {
     double cut2;     // cutoff^2 (FP64, the reference's membership test)
@@ -351,7 +357,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
              const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl,
              DevStatus* st, NlArgs a) {
     __shared__ float4 s_cpos[kNlWarps][kTile];  // candidate relative position, w = slot bits
-    __shared__ int s_cref[kNlWarps][kTile];
+    __shared__ int s_cref[kNlWarps][HM ? kTile : 1];  // root reference indices (half modes only)
     __shared__ int s_crbk[kNlWarps][kTile];
     __shared__ float4 s_hpos[kNlWarps][kHomeMax];
     __shared__ int s_hcnt[kNlWarps][kHomeMax];
@@ -424,7 +430,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 double4 p = pos[slot];
                 s_cpos[wid][m - t0] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]),
                                                   (float)(p.z - ctr[2]), __int_as_float(slot));
-                s_cref[wid][m - t0] = HM ? ref[slot] : 0;  // root reference index (ref for locals)
+                if (HM) s_cref[wid][m - t0] = ref[slot];  // root reference index (ref for locals)
                 s_crbk[wid][m - t0] = rel_cell(rbk[slot], rb0);
             }
             __syncwarp();
@@ -453,7 +459,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                         // core/neighborlist.impala:34: half lists keep i > j (reference index);
                         // HM == 2 compares ghosts by their root so pairs across the
                         // periodic boundary are kept once
-                        pred = in && slot != i && (!HM || s_cref[wid][q] < iref);
+                        pred = in && slot != i && (!HM || s_cref[wid][HM ? q : 0] < iref);
                         if (pred) {
                             // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow
                             // shows up as bits above bit 1 or in byte 3) means |dk| > 1
@@ -658,7 +664,7 @@ void run_distribute(State& s) {
     const int np = 1 - s.pc, nv = 1 - s.vc, na = 1 - s.ac;
     k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
         s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
-        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk, s.bin_cell, s.slot_cell, s.pos32, NA, N, a,
+        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk, s.bin_cell, s.slot_cell, s.pos32.b[np], NA, N, a,
         s.precision);
     launched(K_BIN);
     s.pc = np;

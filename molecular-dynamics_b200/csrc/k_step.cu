@@ -71,6 +71,21 @@ __device__ __forceinline__ void prefetch_list_rows(const uint32_t* nbl, int n, i
     }
 }
 
+// this block's share of a per-slot array (bytes a multiple of 16), prefetched into L2 by
+// warp 0 in pieces of at most 4 KiB: the gathered neighbour positions and the block's own
+// rows arrive at DRAM bandwidth instead of on first touch (cold L2 after other work)
+__device__ __forceinline__ void prefetch_share(const void* base, size_t bytes) {
+    if (threadIdx.x >= 32 || bytes == 0) return;
+    const size_t share = ((bytes + gridDim.x - 1) / gridDim.x + 15) & ~(size_t)15;
+    const size_t lo = share * blockIdx.x;
+    if (lo >= bytes) return;
+    const size_t hi = min(bytes, lo + share);
+    for (size_t o = lo + (size_t)threadIdx.x * 4096; o < hi; o += (size_t)32 * 4096) {
+        const unsigned len = (unsigned)min((size_t)4096, hi - o);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)base + o), "r"(len) : "memory");
+    }
+}
+
 // target of the reaction force of a half-list pair: the local itself or a ghost's root
 __device__ __forceinline__ int reaction_slot(int j, int N, const int* groot) { return j < N ? j : groot[j - N]; }
 
@@ -84,18 +99,31 @@ __device__ __forceinline__ int reaction_slot(int j, int N, const int* groot) { r
 #ifndef TMD_MINB
 #define TMD_MINB (1024 / TMD_THREADS)  // caps registers at 64 per thread
 #endif
+// v += dt/2 f; x += dt v (core/compute.impala:175-184) in the reference's operand order
+__device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, double fx, double fy, double fz,
+                                                 double dt, double h) {
+    v.x = dadd(v.x, dmul(fx, h));
+    v.y = dadd(v.y, dmul(fy, h));
+    v.z = dadd(v.z, dmul(fz, h));
+    return make_double4(dadd(x.x, dmul(v.x, dt)), dadd(x.y, dmul(v.y, dt)), dadd(x.z, dmul(v.z, dt)), x.w);
+}
+
 constexpr int kB64 = TMD_B64;  // neighbours loaded per batch (FP64)
 constexpr int kB32 = TMD_B32;  // neighbours loaded per batch (mixed)
 
-template <bool HALF, bool FUSE, bool THERMO>
+// INIT (with FUSE, full lists): the epilogue also does the next step's initial integration
+// and writes the atom's new position to pos_n, the other buffer (neighbours read pos)
+template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
 __global__ void __launch_bounds__(kThreads)
 k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* __restrict__ vel,
           const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot,
-          double* __restrict__ part, LjArgs a) {
+          double* __restrict__ part, LjArgs a, double4* __restrict__ pos_n = nullptr) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_list_rows(nbl, n, a.stride, a.nbcap);
+    prefetch_share(pos, (size_t)a.NA * sizeof(double4));
+    if (FUSE) prefetch_share(vel, (size_t)a.N * sizeof(double4));
     double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
     if (i < a.N) {
         const double4 pi = pos[i];
@@ -147,8 +175,13 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
                 v.x = dadd(v.x, dmul(fx, a.h));
                 v.y = dadd(v.y, dmul(fy, a.h));
                 v.z = dadd(v.z, dmul(fz, a.h));
-                vel[i] = v;
                 if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
+                if (INIT) {  // positions carry w = 0
+                    double4 x = integrate_one(pi, v, fx, fy, fz, a.dt_i, a.h_i);
+                    x.w = 0.0;
+                    pos_n[i] = x;
+                }
+                vel[i] = v;
             }
         }
     }
@@ -191,15 +224,20 @@ __device__ __forceinline__ void fp64_lj(const double4& pi, int j, const double4*
 // closer than sigma (large forces, ~0.2 per atom in a dense LJ liquid) and
 // pairs within 1e-3 of the cutoff take the FP64 path, so list membership and
 // the cutoff test stay exactly the FP64 decisions.
-template <bool HALF, bool FUSE, bool THERMO>
+template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
 __global__ void __launch_bounds__(kThreads, TMD_MINB)
 k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
            double4* __restrict__ vel, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
-           const int* __restrict__ groot, double* __restrict__ part, LjArgs a) {
+           const int* __restrict__ groot, double* __restrict__ part, LjArgs a,
+           double4* __restrict__ pos_n = nullptr, float4* __restrict__ pos32_n = nullptr,
+           const int* __restrict__ rbk = nullptr) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_list_rows(nbl, n, a.stride, a.nbcap);
+    prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
+    prefetch_share(pos, (size_t)a.N * sizeof(double4));
+    if (FUSE) prefetch_share(vel, (size_t)a.N * sizeof(double4));
     double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
     if (i < a.N) {
         const float4 ri = pos32[i];
@@ -305,8 +343,14 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                 v.x += (double)F.x * a.h;
                 v.y += (double)F.y * a.h;
                 v.z += (double)F.z * a.h;
-                vel[i] = v;
                 if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
+                if (INIT) {  // as k_integrate does it, from the FP32 force
+                    double4 x = integrate_one(pi, v, (double)F.x, (double)F.y, (double)F.z, a.dt_i, a.h_i);
+                    x.w = 0.0;  // positions carry w = 0
+                    pos_n[i] = x;
+                    pos32_n[i] = rebased32(x, rbk[i], a.alo, a.rb_h);
+                }
+                vel[i] = v;
             }
         }
         if (THERMO) {
@@ -511,13 +555,6 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
 //         ghost source still holds the previous step's value (so chained
 //         edge / corner ghosts lag, exactly like comm/comm.impala:334-388);
 //     2 = exact periodic images: ghost = integrated root + total shift.
-__device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, double fx, double fy, double fz,
-                                                 double dt, double h) {
-    v.x = dadd(v.x, dmul(fx, h));
-    v.y = dadd(v.y, dmul(fy, h));
-    v.z = dadd(v.z, dmul(fz, h));
-    return make_double4(dadd(x.x, dmul(v.x, dt)), dadd(x.y, dmul(v.y, dt)), dadd(x.z, dmul(v.z, dt)), x.w);
-}
 
 template <bool MIXED>
 __device__ __forceinline__ void load_force(const double4* frc, const float4* frc32, int i, double& fx, double& fy,
@@ -535,8 +572,8 @@ template <int GM, bool MIXED, bool DEMV>
 __global__ void __launch_bounds__(kThreads)
 k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, const double4* __restrict__ vel_o,
             double4* __restrict__ vel_n, const double4* __restrict__ frc, const float4* __restrict__ frc32,
-            float4* __restrict__ pos32, const int* __restrict__ rbk, const int* __restrict__ gsrc,
-            const int* __restrict__ groot, const int* __restrict__ gcode, StepArgs a) {
+            const float4* __restrict__ pos32_o, float4* __restrict__ pos32_n, const int* __restrict__ rbk,
+            const int* __restrict__ gsrc, const int* __restrict__ groot, const int* __restrict__ gcode, StepArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < a.N) {
         double4 v = vel_o[t];
@@ -545,13 +582,14 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
         const double4 x = integrate_one(pos_o[t], v, fx, fy, fz, a.dt, a.h);
         pos_n[t] = x;
         vel_n[t] = v;
-        if (MIXED) pos32[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
+        if (MIXED) pos32_n[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
         return;
     }
     if (t >= a.N + a.G) return;
     const int g = t - a.N;
     if (GM == 0) {
         pos_n[t] = pos_o[t];
+        if (MIXED) pos32_n[t] = pos32_o[t];
         if (DEMV) vel_n[t] = vel_o[t];
         return;
     }
@@ -573,7 +611,7 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
     x.z = dadd(xs.z, dmul(a.len[2], (double)shift_axis(code, base, 2)));
     x.w = 0.0;
     pos_n[t] = x;
-    if (MIXED) pos32[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
+    if (MIXED) pos32_n[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
     if (DEMV) {  // contact-fixed DEM: ghost velocity = its root's, after this half-kick
         const int r = groot[g];
         double4 vr = vel_o[r];
@@ -589,12 +627,14 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
 // stand-alone ghost refresh (no pending integration): locals carried over
 template <int GM, bool MIXED>
 __global__ void __launch_bounds__(kThreads)
-k_ghost_sync(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, float4* __restrict__ pos32,
-             double4* __restrict__ vel, int demv, const int* __restrict__ rbk, const int* __restrict__ gsrc,
-             const int* __restrict__ groot, const int* __restrict__ gcode, StepArgs a) {
+k_ghost_sync(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, const float4* __restrict__ pos32_o,
+             float4* __restrict__ pos32_n, double4* __restrict__ vel, int demv, const int* __restrict__ rbk,
+             const int* __restrict__ gsrc, const int* __restrict__ groot, const int* __restrict__ gcode,
+             StepArgs a) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < a.N) {
         pos_n[t] = pos_o[t];
+        if (MIXED) pos32_n[t] = pos32_o[t];
         return;
     }
     if (t >= a.N + a.G) return;
@@ -609,8 +649,38 @@ k_ghost_sync(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, flo
     x.z = dadd(xs.z, dmul(a.len[2], (double)shift_axis(code, base, 2)));
     x.w = 0.0;
     pos_n[t] = x;
-    if (MIXED) pos32[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
+    if (MIXED) pos32_n[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
     if (demv) vel[t] = vel[groot[g]];  // ghost slots only; roots are locals
+}
+
+// ghosts after a force kernel that also did the next initial integration of the locals
+// (k_lj_*<.., INIT>): pos_n/pos32_n hold the new locals, pos_o the previous buffer.
+// GM 0 carries the ghosts over; 1 and 2 give exactly what k_integrate<1|2> computes, since
+// the new local equals its on-the-fly integration there.
+template <int GM, bool MIXED>
+__global__ void __launch_bounds__(kThreads)
+k_ghost_refresh(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, const float4* __restrict__ pos32_o,
+                float4* __restrict__ pos32_n, const int* __restrict__ rbk, const int* __restrict__ gsrc,
+                const int* __restrict__ groot, const int* __restrict__ gcode, StepArgs a) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= a.G) return;
+    const int t = a.N + g;
+    if (GM == 0) {
+        pos_n[t] = pos_o[t];
+        if (MIXED) pos32_n[t] = pos32_o[t];
+        return;
+    }
+    const int code = gcode[g];
+    const int s = GM == 1 ? gsrc[g] : groot[g];
+    const double4 xs = s < a.N ? pos_n[s] : pos_o[s];
+    const int base = GM == 1 ? 0 : 8;
+    double4 x;
+    x.x = dadd(xs.x, dmul(a.len[0], (double)shift_axis(code, base, 0)));
+    x.y = dadd(xs.y, dmul(a.len[1], (double)shift_axis(code, base, 1)));
+    x.z = dadd(xs.z, dmul(a.len[2], (double)shift_axis(code, base, 2)));
+    x.w = 0.0;
+    pos_n[t] = x;
+    if (MIXED) pos32_n[t] = rebased32(x, rbk[t], a.alo, a.rb_h);
 }
 
 template <bool MIXED, bool THERMO>
@@ -673,15 +743,18 @@ StepArgs step_args(const State& s, double dt) {
     return a;
 }
 
-template <bool HALF, bool FUSE, bool THERMO>
+// INIT: the kernels write the integrated locals into the other position buffer
+template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
 void launch_lj(State& s, const LjArgs& a, int nb) {
     double4* vel = s.vel.b[s.vc];
+    double4* pn = INIT ? s.pos.b[1 - s.pc] : nullptr;
     if (s.precision == 1)
-        k_lj_mixed<HALF, FUSE, THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos32, s.pos.b[s.pc], s.frc32, vel, s.nbn,
-                                                                     s.nbl, s.groot, s.red_part, a);
+        k_lj_mixed<HALF, FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(
+            s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, vel, s.nbn, s.nbl, s.groot, s.red_part, a, pn,
+            INIT ? s.pos32.b[1 - s.pc] : nullptr, s.rbk);
     else
-        k_lj_fp64<HALF, FUSE, THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn, s.nbl,
-                                                                    s.groot, s.red_part, a);
+        k_lj_fp64<HALF, FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn,
+                                                                          s.nbl, s.groot, s.red_part, a, pn);
 }
 
 }  // namespace
@@ -754,6 +827,56 @@ void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
     }
 }
 
+bool force_init_fusable(const State& s, const PendingForce& p) {
+    // ghost velocities of the contact-fixed DEM model come from k_integrate
+    return !p.dem && !p.half && !s.lists_half && s.dem_fixed == 0 && !(s.precision == 1 && s.tiles_valid);
+}
+
+void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double dt_init) {
+    const int N = s.N;
+    if (N == 0) return;  // no ghosts either
+    LjArgs a = lj_args(s, p, dt_final);
+    a.hx = (float)(-s.geo.rb_h);
+    a.hy = (float)(-s.geo.rb_h / 4.0);
+    a.hz = (float)(-s.geo.rb_h / 16.0);
+    a.dt_i = dt_init;
+    a.h_i = 0.5 * dt_init;
+    const int nb = nblocks(N, kThreads);
+    const bool thermo = s.thermo != 0;
+    if (thermo) ensure_red_scratch(s, kThermoQ * nb);
+    prof_begin(K_FORCE_LJ);
+    if (thermo) launch_lj<false, true, true, true>(s, a, nb);
+    else launch_lj<false, true, false, true>(s, a, nb);
+    launched(K_FORCE_LJ);
+    prof_end(K_FORCE_LJ);
+    s.pc = 1 - s.pc;  // the locals of the other buffer are current; its ghosts follow
+    s.integration_iters = N;
+    if (thermo) {
+        k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 0, kThermoQ);
+        launched(K_REDUCE);
+    }
+}
+
+void run_ghost_refresh(State& s, int gm) {
+    if (s.G == 0) return;
+    StepArgs a = step_args(s, 0.0);
+    const double4* po = s.pos.b[1 - s.pc];
+    double4* pn = s.pos.b[s.pc];
+    const float4* p32o = s.pos32.b[1 - s.pc];
+    float4* p32n = s.pos32.b[s.pc];
+    const int nb = nblocks(s.G, kThreads);
+    const bool mixed = s.precision == 1;
+#define TMD_GR(GM_, MX_) \
+    k_ghost_refresh<GM_, MX_><<<nb, kThreads, 0, s.stream>>>(po, pn, p32o, p32n, s.rbk, s.gsrc, s.groot, s.gcode, a)
+    prof_begin(K_GHOST_SYNC);
+    if (gm == 0) { if (mixed) TMD_GR(0, true); else TMD_GR(0, false); }
+    else if (gm == 1) { if (mixed) TMD_GR(1, true); else TMD_GR(1, false); }
+    else { if (mixed) TMD_GR(2, true); else TMD_GR(2, false); }
+#undef TMD_GR
+    launched(K_GHOST_SYNC);
+    prof_end(K_GHOST_SYNC);
+}
+
 void run_force_dem(State& s, const PendingForce& p) {
     const int N = s.N;
     if (N == 0) return;
@@ -790,10 +913,10 @@ void run_force_dem(State& s, const PendingForce& p) {
         prof_begin(K_FORCE_DEM);
         if (p.half)
             k_dem_mixed<true><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(
-                s.pos32, s.pos.b[s.pc], s.vel.b[s.vc], s.frc32, s.nbn, s.nbl, s.groot, a, b);
+                s.pos32.b[s.pc], s.pos.b[s.pc], s.vel.b[s.vc], s.frc32, s.nbn, s.nbl, s.groot, a, b);
         else
             k_dem_mixed<false><<<nblocks(N, kThreads), kThreads, 0, s.stream>>>(
-                s.pos32, s.pos.b[s.pc], s.vel.b[s.vc], s.frc32, s.nbn, s.nbl, s.groot, a, b);
+                s.pos32.b[s.pc], s.pos.b[s.pc], s.vel.b[s.vc], s.frc32, s.nbn, s.nbl, s.groot, a, b);
         launched(K_FORCE_DEM);
         prof_end(K_FORCE_DEM);
         return;
@@ -824,9 +947,11 @@ void run_integrate(State& s, double dt, bool fuse_ghosts) {
     double4* pn = s.pos.b[1 - s.pc];
     const double4* vo = s.vel.b[s.vc];
     double4* vn = s.vel.b[1 - s.vc];
+    const float4* p32o = s.pos32.b[s.pc];
+    float4* p32n = s.pos32.b[1 - s.pc];
     const int nb = nblocks(NA, kThreads);
 #define TMD_INT(GM_, MX_, DV_)                                                                                 \
-    k_integrate<GM_, MX_, DV_><<<nb, kThreads, 0, s.stream>>>(po, pn, vo, vn, s.frc.b[s.ac], s.frc32, s.pos32, \
+    k_integrate<GM_, MX_, DV_><<<nb, kThreads, 0, s.stream>>>(po, pn, vo, vn, s.frc.b[s.ac], s.frc32, p32o, p32n,  \
                                                               s.rbk, s.gsrc, s.groot, s.gcode, a)
     prof_begin(K_INTEGRATE);
     if (gm == 0) {
@@ -853,14 +978,16 @@ void run_ghost_sync(State& s) {
     StepArgs a = step_args(s, 0.0);
     const double4* po = s.pos.b[s.pc];
     double4* pn = s.pos.b[1 - s.pc];
+    const float4* p32o = s.pos32.b[s.pc];
+    float4* p32n = s.pos32.b[1 - s.pc];
     const int nb = nblocks(NA, kThreads);
     prof_begin(K_GHOST_SYNC);
     if (s.ghost_exact) {
-        if (s.precision == 1) k_ghost_sync<2, true><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
-        else k_ghost_sync<2, false><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+        if (s.precision == 1) k_ghost_sync<2, true><<<nb, kThreads, 0, s.stream>>>(po, pn, p32o, p32n, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+        else k_ghost_sync<2, false><<<nb, kThreads, 0, s.stream>>>(po, pn, p32o, p32n, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
     } else {
-        if (s.precision == 1) k_ghost_sync<1, true><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
-        else k_ghost_sync<1, false><<<nb, kThreads, 0, s.stream>>>(po, pn, s.pos32, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+        if (s.precision == 1) k_ghost_sync<1, true><<<nb, kThreads, 0, s.stream>>>(po, pn, p32o, p32n, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
+        else k_ghost_sync<1, false><<<nb, kThreads, 0, s.stream>>>(po, pn, p32o, p32n, s.vel.b[s.vc], s.dem_fixed, s.rbk, s.gsrc, s.groot, s.gcode, a);
     }
     launched(K_GHOST_SYNC);
     prof_end(K_GHOST_SYNC);
@@ -895,7 +1022,7 @@ void run_refresh_pos32(State& s) {
     const int NA = s.N + s.G;
     if (NA == 0) return;
     StepArgs a = step_args(s, 0.0);
-    k_refresh_pos32<<<nblocks(NA, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.pos32, s.rbk, NA, a);
+    k_refresh_pos32<<<nblocks(NA, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.pos32.b[s.pc], s.rbk, NA, a);
     launched(K_MISC);
 }
 

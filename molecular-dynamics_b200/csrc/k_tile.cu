@@ -737,7 +737,7 @@ void run_force_lj_tiles(State& s, const PendingForce& p, bool fuse_final, double
                                           (int)smem));                                                             \
             smem_set = smem;                                                                                       \
         }                                                                                                          \
-        k_lj_tile_mixed<F, T><<<nb, kBlockHomes, smem, s.stream>>>(s.pos32, s.pos.b[s.pc], s.frc32, vel, s.nbn,   \
+        k_lj_tile_mixed<F, T><<<nb, kBlockHomes, smem, s.stream>>>(s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, vel, s.nbn,   \
                                                                    s.tile_stream, s.tile_desc, s.red_part, a);    \
     } while (0)
     if (fuse_final) {

@@ -8,8 +8,10 @@
 namespace tmd {
 
 struct LjArgs {
-    int N, stride, nbcap;
+    int N, NA, stride, nbcap;  // NA = locals + ghosts
     double rc2, sigma6, eps, h;
+    double dt_i, h_i;          // the next step's initial integration (fused kernels only)
+    double alo[3], rb_h;       // rebasing grid (mixed form's positions)
     // mixed form
     float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f;
     float hx, hy, hz;  // shift decode scales (see the kernels)
@@ -29,12 +31,16 @@ inline double ipow(double x, int n) {
 inline LjArgs lj_args(const State& s, const PendingForce& p, double dt) {
     LjArgs a;
     a.N = s.N;
+    a.NA = s.N + s.G;
     a.stride = s.nb_stride;
     a.nbcap = s.nb_cap;
     a.rc2 = p.rc * p.rc;
     a.sigma6 = ipow(p.sigma, 6);
     a.eps = p.eps;
     a.h = 0.5 * dt;
+    a.dt_i = a.h_i = 0.0;
+    for (int d = 0; d < 3; ++d) a.alo[d] = s.geo.aabb_lo[d];
+    a.rb_h = s.geo.rb_h;
     // FP32 rsq of a list pair is within ~4e-6 of the FP64 value (del components
     // carry at most ~3.6e-7 error); pairs inside this window take the FP64 test
     const double margin = 2e-5 * a.rc2 + 1e-7;

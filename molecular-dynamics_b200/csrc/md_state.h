@@ -97,7 +97,7 @@ struct State {
     DBuf<double4> vel;   int vc = 0;   // velocities
     DBuf<double4> frc;   DBuf<double> mass;  DBuf<int> ref;  DBuf<int> img;  int ac = 0;
     float4* frc32 = nullptr;   // mixed-form forces
-    float4* pos32 = nullptr;   // mixed-form rebased positions
+    DBuf<float4> pos32;        // mixed-form rebased positions, double-buffered with pos (index pc)
     int* rbk = nullptr;        // packed rebasing cell of each slot
     int* slot_of_ref = nullptr;
     int* rref = nullptr;       // per slot: reference index of the root local (= ref for locals)
@@ -151,6 +151,13 @@ struct State {
     PendingForce force_cfg;   // parameters of the last md_compute_* call
     bool pend_init = false;
     double pend_dt = 0.0;
+    // a full-list LJ force whose final integration was requested: launched when the next
+    // call is known, fused with the next step's initial integration when that is the call
+    bool pend_final = false;
+    double pend_final_dt = 0.0;
+    PendingForce final_cfg;
+    // locals were integrated by that fused kernel; ghosts still to be refreshed or carried
+    bool pend_ghost = false;
 
     // reported iteration counters (core/runtime.impala:3-5)
     long long force_iters = 0, rsq_iters = 0, integration_iters = 0;
@@ -198,6 +205,14 @@ void run_integrate(State& s, double dt, bool fuse_ghosts);
 void run_ghost_sync(State& s);
 void run_final(State& s, double dt);
 void run_refresh_pos32(State& s);
+// the LJ force (full list) with the final kick of dt_final and the next step's initial
+// integration of dt_init fused into its epilogue (plain-list kernels); writes the locals of
+// the other position buffer, which becomes current (ghosts: run_ghost_refresh)
+void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double dt_init);
+bool force_init_fusable(const State& s, const PendingForce& p);
+// ghosts of the current buffer from their sources after run_force_lj_init: gm 0 carries
+// them over, 1 is the reference two-phase refresh, 2 exact images
+void run_ghost_refresh(State& s, int gm);
 void run_reduce_thermo(State& s, int nblocks, int nq);
 // sums the [q][nblocks] per-block partials of quantities q0..q1-1 into thermo_dev[q]
 void run_reduce_partials(State& s, int nblocks, int q0, int q1);
