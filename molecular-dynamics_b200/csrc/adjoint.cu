@@ -11,7 +11,7 @@
 //   a_x += c J(x_{t+1}) a_v ; a_v += dt a_x ; a_x += c J(x_t) a_v ; (theta: c dF/dtheta^T a_v at both)
 // where J = dF/dx = -Hessian.  The product J(x_t) a_v(t) appears in step t
 // (initial kick) and step t-1 (final kick), so one Hessian-vector product per
-// step suffices: k_adj_hvp computes u = J(x_t) a_v, adds dt*u (c*u at t = 0)
+// step suffices: k_adj_hvp_split computes u = J(x_t) a_v, adds dt*u (c*u at t = 0)
 // to a_x, applies the next drift a_v += dt a_x, and accumulates the theta
 // terms with weight dt (c at t = 0) into per-block sums (deterministic).
 //
@@ -59,7 +59,9 @@ double4* ck_x = nullptr;   // [nseg][N] positions, reference order
 double4* ck_v = nullptr;   // [nseg][N] velocities
 int* ck_img = nullptr;     // [nseg][N] wrap counts
 double4* x0_dev = nullptr; // [N] initial positions, reference order
-double4* seg_x = nullptr;  // [reneigh][N] local positions of one segment, slot order
+double4* seg_x = nullptr;  // [reneigh][N + G] positions (ghosts too) of one segment, slot order
+int* nbr = nullptr;        // root slot of each list entry, laid out as the list
+size_t cap_nbr = 0;
 double4* ax = nullptr;     // [N] adjoint of positions, slot order
 double4* av[2] = {nullptr, nullptr};
 double4* tmp4 = nullptr;   // [N] reference-order staging
@@ -82,53 +84,83 @@ struct HvpArgs {
 // f = 48 eps sr6 (sr6 - 1/2) sr2, f' = df/ds = 48 eps sr2^2 sr6 (2 - 7 sr6);
 // theta terms: w_i . F_i / eps and sum_j df/dsigma (d . w_i),
 // df/dsigma = (144 eps / sigma) sr2 sr6 (4 sr6 - 1).
+// The neighbour loop is split over kLpa adjacent lanes per atom (lane
+// `sub` takes entries sub, sub + kLpa, ...) in batches of kHb with the next batch's
+// entries loaded ahead, and the lanes' sums combined by shuffles.  Ghost neighbours
+// read their stored position (xs holds all slots of the step) and the adjoint of
+// their root through the root list `nbr`, so a neighbour costs two independent gathers.
+constexpr int kLpa = 4;  // lanes per atom
+constexpr int kHb = 2;   // neighbours per lane per batch
+
 __global__ void __launch_bounds__(kT)
-k_adj_hvp(const double4* __restrict__ xs, const double4* __restrict__ w, double4* __restrict__ w_next,
-          double4* __restrict__ ax, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
-          const int* __restrict__ groot, const int* __restrict__ gcode, double* __restrict__ gacc, HvpArgs a) {
+k_adj_hvp_split(const double4* __restrict__ xs, const double4* __restrict__ w, double4* __restrict__ w_next,
+                double4* __restrict__ ax, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
+                const int* __restrict__ nbr, double* __restrict__ gacc, HvpArgs a) {
     __shared__ double scratch[kT / 32];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double ge = 0.0, gs = 0.0;
-    if (i < a.N) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t / kLpa, sub = t % kLpa;
+    const bool act = i < a.N;
+    double ux = 0.0, uy = 0.0, uz = 0.0, Fx = 0.0, Fy = 0.0, Fz = 0.0, gs = 0.0;
+    double4 wi = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (act) {
         const double4 xi = xs[i];
-        const double4 wi = w[i];
-        double ux = 0.0, uy = 0.0, uz = 0.0, Fx = 0.0, Fy = 0.0, Fz = 0.0;
+        wi = w[i];
         const int n = min(nbn[i], a.nbcap);
-        for (int k = 0; k < n; ++k) {
-            const int j = (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits);
-            double4 xj, wj;
-            if (j < a.N) {
-                xj = xs[j];
-                wj = w[j];
-            } else {
-                const int g = j - a.N;
-                const int r = groot[g];
-                const int code = gcode[g];
-                xj = xs[r];
-                xj.x += a.len[0] * shift_axis(code, 8, 0);
-                xj.y += a.len[1] * shift_axis(code, 8, 1);
-                xj.z += a.len[2] * shift_axis(code, 8, 2);
-                wj = w[r];
+        int ej[kHb], er[kHb];
+#pragma unroll
+        for (int b = 0; b < kHb; ++b) {
+            const int k = sub + b * kLpa;
+            ej[b] = k < n ? (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits) : i;
+            er[b] = k < n ? __ldg(nbr + (size_t)k * a.stride + i) : i;
+        }
+        for (int k0 = sub; k0 < n; k0 += kLpa * kHb) {
+            double4 xj[kHb], wj[kHb];
+#pragma unroll
+            for (int b = 0; b < kHb; ++b) {
+                xj[b] = xs[ej[b]];
+                wj[b] = w[er[b]];
             }
-            const double dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
-            const double s = dx * dx + dy * dy + dz * dz;
-            if (s < a.rc2) {
-                const double sr2 = 1.0 / s;
-                const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
-                const double f = 48.0 * a.eps * sr6 * (sr6 - 0.5) * sr2;
-                const double fp = 48.0 * a.eps * sr2 * sr2 * sr6 * (2.0 - 7.0 * sr6);
-                const double wx = wi.x - wj.x, wy = wi.y - wj.y, wz = wi.z - wj.z;
-                const double dw = 2.0 * fp * (dx * wx + dy * wy + dz * wz);
-                ux += f * wx + dw * dx;
-                uy += f * wy + dw * dy;
-                uz += f * wz + dw * dz;
-                Fx += f * dx;
-                Fy += f * dy;
-                Fz += f * dz;
-                gs += 144.0 * a.eps * a.inv_sigma * sr2 * sr6 * (4.0 * sr6 - 1.0) *
-                      (dx * wi.x + dy * wi.y + dz * wi.z);
+#pragma unroll
+            for (int b = 0; b < kHb; ++b) {
+                const int k = k0 + kLpa * kHb + b * kLpa;
+                ej[b] = k < n ? (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits) : i;
+                er[b] = k < n ? __ldg(nbr + (size_t)k * a.stride + i) : i;
+            }
+#pragma unroll
+            for (int b = 0; b < kHb; ++b) {
+                if (k0 + b * kLpa >= n) continue;
+                const double dx = xi.x - xj[b].x, dy = xi.y - xj[b].y, dz = xi.z - xj[b].z;
+                const double s = dx * dx + dy * dy + dz * dz;
+                if (s < a.rc2) {
+                    const double sr2 = 1.0 / s;
+                    const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
+                    const double f = 48.0 * a.eps * sr6 * (sr6 - 0.5) * sr2;
+                    const double fp = 48.0 * a.eps * sr2 * sr2 * sr6 * (2.0 - 7.0 * sr6);
+                    const double wx = wi.x - wj[b].x, wy = wi.y - wj[b].y, wz = wi.z - wj[b].z;
+                    const double dw = 2.0 * fp * (dx * wx + dy * wy + dz * wz);
+                    ux += f * wx + dw * dx;
+                    uy += f * wy + dw * dy;
+                    uz += f * wz + dw * dz;
+                    Fx += f * dx;
+                    Fy += f * dy;
+                    Fz += f * dz;
+                    gs += 144.0 * a.eps * a.inv_sigma * sr2 * sr6 * (4.0 * sr6 - 1.0) *
+                          (dx * wi.x + dy * wi.y + dz * wi.z);
+                }
             }
         }
+    }
+#pragma unroll
+    for (int o = 1; o < kLpa; o <<= 1) {
+        ux += __shfl_xor_sync(0xffffffffu, ux, o);
+        uy += __shfl_xor_sync(0xffffffffu, uy, o);
+        uz += __shfl_xor_sync(0xffffffffu, uz, o);
+        Fx += __shfl_xor_sync(0xffffffffu, Fx, o);
+        Fy += __shfl_xor_sync(0xffffffffu, Fy, o);
+        Fz += __shfl_xor_sync(0xffffffffu, Fz, o);
+    }
+    double ge = 0.0;
+    if (act && sub == 0) {
         ge = (wi.x * Fx + wi.y * Fy + wi.z * Fz) / a.eps;
         double4 q = ax[i];
         q.x += a.kick * ux;
@@ -142,6 +174,18 @@ k_adj_hvp(const double4* __restrict__ xs, const double4* __restrict__ w, double4
     if (threadIdx.x == 0) {
         gacc[blockIdx.x] += a.wt * se;
         gacc[gridDim.x + blockIdx.x] += a.wt * ss;
+    }
+}
+
+// the root slot of every list entry (a ghost's root local, a local itself)
+__global__ void k_root_list(const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
+                            const int* __restrict__ groot, int* __restrict__ nbr, int N, int stride, int nbcap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int n = min(nbn[i], nbcap);
+    for (int k = 0; k < n; ++k) {
+        const int j = (int)(nbl[(size_t)k * stride + i] >> kCodeBits);
+        nbr[(size_t)k * stride + i] = j < N ? j : groot[j - N];
     }
 }
 
@@ -257,9 +301,10 @@ void ensure(T** p, int& cap, size_t need) {
 }
 
 void free_adjoint() {
-    dfree(&ck_x); dfree(&ck_v); dfree(&ck_img); dfree(&x0_dev); dfree(&seg_x); dfree(&ax);
+    dfree(&ck_x); dfree(&ck_v); dfree(&ck_img); dfree(&x0_dev); dfree(&seg_x); dfree(&nbr); dfree(&ax);
     dfree(&av[0]); dfree(&av[1]); dfree(&tmp4); dfree(&gacc); dfree(&red); dfree(&mass_ref);
     cap_n = cap_seg = cap_ck = 0;
+    cap_nbr = 0;
 }
 
 // the list and layout for positions at the start of a segment (already wrapped)
@@ -359,21 +404,14 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     run.sigma = sigma;
     run.nseg = (cfg.steps + cfg.reneigh - 1) / cfg.reneigh;
     ensure(&ck_x, cap_ck, (size_t)run.nseg * N);
-    {
-        int c1 = 0, c2 = 0;
-        dfree(&ck_v);
-        dfree(&ck_img);
-        dalloc(&ck_v, (size_t)run.nseg * N);
-        dalloc(&ck_img, (size_t)run.nseg * N);
-        (void)c1;
-        (void)c2;
-    }
-    int cap_tmp = 0;
+    dfree(&ck_v);
+    dfree(&ck_img);
+    dalloc(&ck_v, (size_t)run.nseg * N);
+    dalloc(&ck_img, (size_t)run.nseg * N);
     dfree(&x0_dev);
     dalloc(&x0_dev, N);
     dfree(&mass_ref);
     dalloc(&mass_ref, N);
-    (void)cap_tmp;
     // initial state in reference order: x_0 from md_initialize_grid, v_0 from the caller
     std::vector<double4> hx(N), hv(N);
     for (int i = 0; i < N; ++i) {
@@ -403,7 +441,6 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     cudaEventRecord(e1, s.stream);
     // loss: MSD and U at x_T, and the initial adjoint state
     const int nb = nblk(N);
-    int capd = 0;
     dfree(&ax);
     dalloc(&ax, N);
     dfree(&av[0]);
@@ -413,10 +450,10 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     dfree(&tmp4);
     dalloc(&tmp4, N);
     dfree(&gacc);
-    dalloc(&gacc, 2 * (size_t)nb + 2);
+    const int nbs = nblk(kLpa * N);  // blocks of the reverse pass's product kernel
+    dalloc(&gacc, 2 * (size_t)nbs + 2);
     dfree(&red);
     dalloc(&red, 8);
-    (void)capd;
     ensure_red_scratch(s, 2 * nb);
     const double sig6 = std::pow(sigma, 6);
     k_adj_init<<<nb, kT, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.ref.b[s.ac], x0_dev, s.frc.b[s.ac], s.frc32,
@@ -449,9 +486,9 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     }
     run.loss = sums[0] / N + run.U / N;
     // the direct theta terms of U(x_T)/N; the reverse pass adds the trajectory terms
-    std::vector<double> g0(2 * (size_t)nb + 2, 0.0);
-    g0[2 * (size_t)nb] = run.U / (N * epsilon);
-    g0[2 * (size_t)nb + 1] = dUds / N;
+    std::vector<double> g0(2 * (size_t)nbs + 2, 0.0);
+    g0[2 * (size_t)nbs] = run.U / (N * epsilon);
+    g0[2 * (size_t)nbs + 1] = dUds / N;
     TMD_CUDA(cudaMemcpyAsync(gacc, g0.data(), sizeof(double) * g0.size(), cudaMemcpyHostToDevice, s.stream));
     // adjoint state to reference order (the backward pass starts in another layout)
     k_to_ref<<<nb, kT, 0, s.stream>>>(ax, s.ref.b[s.ac], tmp4, N);
@@ -475,12 +512,8 @@ int md_adjoint_backward(double* grad_v0, double* grad_eps, double* grad_sigma) {
     }
     const int N = s.N;
     const int nb = nblk(N);
+    const int nbs = nblk(kLpa * N);
     const int R = cfg.reneigh;
-    if (cap_seg < R * N || !seg_x) {
-        dfree(&seg_x);
-        dalloc(&seg_x, (size_t)R * N);
-        cap_seg = R * N;
-    }
     ModeGuard guard(s);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -493,11 +526,26 @@ int md_adjoint_backward(double* grad_v0, double* grad_eps, double* grad_sigma) {
         const int t1 = std::min(t0 + R, cfg.steps);  // positions x_t0 .. x_{t1-1}
         reset_identity(s, seg);
         rebuild(s);
+        // this segment's slots (ghosts included) and its root list
+        const int NA = N + s.G;
+        if ((size_t)cap_seg < (size_t)R * NA || !seg_x) {
+            dfree(&seg_x);
+            cap_seg = R * (NA + NA / 8 + 256);
+            dalloc(&seg_x, (size_t)cap_seg);
+        }
+        const size_t nl = (size_t)s.nb_cap * s.nb_stride;
+        if (cap_nbr < nl || !nbr) {
+            dfree(&nbr);
+            dalloc(&nbr, nl);
+            cap_nbr = nl;
+        }
+        k_root_list<<<nb, kT, 0, s.stream>>>(s.nbn, s.nbl, s.groot, nbr, N, s.nb_stride, s.nb_cap);
+        launched(K_ADJ_STEP);
         run_force_lj(s, force_params(), false, 0.0);
-        TMD_CUDA(cudaMemcpyAsync(seg_x, s.pos.b[s.pc], sizeof(double4) * N, cudaMemcpyDeviceToDevice, s.stream));
+        TMD_CUDA(cudaMemcpyAsync(seg_x, s.pos.b[s.pc], sizeof(double4) * NA, cudaMemcpyDeviceToDevice, s.stream));
         for (int t = t0; t + 1 < t1; ++t) {
             forward_step(s, t, false);
-            TMD_CUDA(cudaMemcpyAsync(seg_x + (size_t)(t + 1 - t0) * N, s.pos.b[s.pc], sizeof(double4) * N,
+            TMD_CUDA(cudaMemcpyAsync(seg_x + (size_t)(t + 1 - t0) * NA, s.pos.b[s.pc], sizeof(double4) * NA,
                                      cudaMemcpyDeviceToDevice, s.stream));
         }
         // adjoint state into this segment's slot order
@@ -522,8 +570,8 @@ int md_adjoint_backward(double* grad_v0, double* grad_eps, double* grad_sigma) {
             a.drift = t > 0 ? cfg.dt : 0.0;
             a.wt = t > 0 ? cfg.dt : c;
             prof_begin(K_HVP);
-            k_adj_hvp<<<nb, kT, 0, s.stream>>>(seg_x + (size_t)(t - t0) * N, av[wcur], av[1 - wcur], ax, s.nbn,
-                                              s.nbl, s.groot, s.gcode, gacc, a);
+            k_adj_hvp_split<<<nbs, kT, 0, s.stream>>>(seg_x + (size_t)(t - t0) * NA, av[wcur], av[1 - wcur], ax,
+                                                      s.nbn, s.nbl, nbr, gacc, a);
             launched(K_HVP);
             prof_end(K_HVP);
             wcur = 1 - wcur;
@@ -537,12 +585,12 @@ int md_adjoint_backward(double* grad_v0, double* grad_eps, double* grad_sigma) {
     }
     cudaEventRecord(e1, s.stream);
     // theta gradients: per-block sums plus the direct terms stored after them
-    k_sum_rows<<<1, 256, 0, s.stream>>>(gacc, red, nb, 2);
+    k_sum_rows<<<1, 256, 0, s.stream>>>(gacc, red, nbs, 2);
     launched(K_ADJ_STEP);
     double gsum[2] = {0, 0}, direct[2] = {0, 0};
     std::vector<double4> hv(N);
     TMD_CUDA(cudaMemcpyAsync(gsum, red, sizeof(gsum), cudaMemcpyDeviceToHost, s.stream));
-    TMD_CUDA(cudaMemcpyAsync(direct, gacc + 2 * (size_t)nb, sizeof(direct), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(direct, gacc + 2 * (size_t)nbs, sizeof(direct), cudaMemcpyDeviceToHost, s.stream));
     TMD_CUDA(cudaMemcpyAsync(hv.data(), av[wcur], sizeof(double4) * N, cudaMemcpyDeviceToHost, s.stream));
     TMD_CUDA(cudaStreamSynchronize(s.stream));
     float bms = 0.f;

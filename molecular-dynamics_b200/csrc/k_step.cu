@@ -129,19 +129,28 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
         const double4 pi = pos[i];
         double fx = 0.0, fy = 0.0, fz = 0.0;
         const uint32_t* lp = nbl + i;
+        const uint32_t pad = (uint32_t)i << kCodeBits;  // the atom itself, skipped below
+        uint32_t ent[kB64];
+#pragma unroll
+        for (int u = 0; u < kB64; ++u) ent[u] = u < n ? __ldg(lp + (size_t)u * a.stride) : pad;
         for (int k0 = 0; k0 < n; k0 += kB64) {
             int j[kB64];
             double4 pj[kB64];
 #pragma unroll
-            for (int u = 0; u < kB64; ++u)
-                j[u] = (k0 + u < n) ? (int)(__ldg(lp + (size_t)(k0 + u) * a.stride) >> kCodeBits) : i;
+            for (int u = 0; u < kB64; ++u) j[u] = (int)(ent[u] >> kCodeBits);
 #pragma unroll
             for (int u = 0; u < kB64; ++u) pj[u] = ldg_d4(pos + j[u]);
+            // the next batch's entries load while this batch's gathers are in flight
 #pragma unroll
             for (int u = 0; u < kB64; ++u) {
-                if (k0 + u >= n) continue;
+                const int q = k0 + kB64 + u;
+                ent[u] = q < n ? __ldg(lp + (size_t)q * a.stride) : pad;
+            }
+#pragma unroll
+            for (int u = 0; u < kB64; ++u) {
                 const double dx = dsub(pi.x, pj[u].x), dy = dsub(pi.y, pj[u].y), dz = dsub(pi.z, pj[u].z);
                 const double rsq = len2_strict(dx, dy, dz);
+                if (k0 + u >= n) continue;
                 if (rsq < a.rc2) {
                     const double sr2 = ddiv(1.0, rsq);
                     const double sr6 = dmul(dmul(dmul(sr2, sr2), sr2), a.sigma6);
@@ -224,28 +233,27 @@ __device__ __forceinline__ void fp64_lj(const double4& pi, int j, const double4*
 // closer than sigma (large forces, ~0.2 per atom in a dense LJ liquid) and
 // pairs within 1e-3 of the cutoff take the FP64 path, so list membership and
 // the cutoff test stay exactly the FP64 decisions.
-template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
+//
+// Half lists: each pair once, the reaction added atomically to j (or to the root of
+// a ghost j); forces must be zeroed before the launch.
+template <bool THERMO>
 __global__ void __launch_bounds__(kThreads, TMD_MINB)
-k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
-           double4* __restrict__ vel, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
-           const int* __restrict__ groot, double* __restrict__ part, LjArgs a,
-           double4* __restrict__ pos_n = nullptr, float4* __restrict__ pos32_n = nullptr,
-           const int* __restrict__ rbk = nullptr) {
+k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
+                const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot,
+                double* __restrict__ part, LjArgs a) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_list_rows(nbl, n, a.stride, a.nbcap);
     prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
     prefetch_share(pos, (size_t)a.N * sizeof(double4));
-    if (FUSE) prefetch_share(vel, (size_t)a.N * sizeof(double4));
-    double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
+    double e = 0.0, w = 0.0, cnt = 0.0;
     if (i < a.N) {
         const float4 ri = pos32[i];
         const double4 pi = pos[i];
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
-        int nq = 0, q0 = 0, q1 = 0;  // deferred FP64 pairs
         const uint32_t* lp = nbl + i;
         for (int k0 = 0; k0 < n; k0 += kB32) {
             uint32_t ent[kB32];
@@ -268,6 +276,7 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                 const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 if (!(rsq < a.rc2_hi)) continue;
                 const int j = (int)(en >> kCodeBits);
+                const int t = reaction_slot(j, a.N, groot);
                 if (rsq < a.rc2_lo && rsq >= a.close2) {
                     float sr2;  // hardware reciprocal (~1 ulp); the error budget is set by del, not by 1/r^2
                     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
@@ -277,18 +286,15 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                     fx += px;
                     fy += py;
                     fz += pz;
-                    if (HALF) {
-                        const int t = reaction_slot(j, a.N, groot);
-                        atomicAdd(&frc32[t].x, -px);
-                        atomicAdd(&frc32[t].y, -py);
-                        atomicAdd(&frc32[t].z, -pz);
-                    }
+                    atomicAdd(&frc32[t].x, -px);
+                    atomicAdd(&frc32[t].y, -py);
+                    atomicAdd(&frc32[t].z, -pz);
                     if (THERMO) {
                         ef += a.eps4f * sr6 * (sr6 - 1.0f);
                         wf += f * rsq;
                         ncnt++;
                     }
-                } else if (HALF) {
+                } else {
                     // FP64 path: exact cutoff decision and close-contact accuracy
                     const double4 pj = ldg_d4(pos + j);
                     const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
@@ -300,7 +306,6 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                         cx += ex * f;
                         cy += ey * f;
                         cz += ez * f;
-                        const int t = reaction_slot(j, a.N, groot);
                         atomicAdd(&frc32[t].x, (float)(-ex * f));
                         atomicAdd(&frc32[t].y, (float)(-ey * f));
                         atomicAdd(&frc32[t].z, (float)(-ez * f));
@@ -310,14 +315,113 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                             ncnt++;
                         }
                     }
-                } else {
-                    // FP64 path, deferred: the pair joins a short queue that is worked off in
-                    // list order after the loop (or when full), so a warp's rare FP64 pairs run
-                    // together instead of each stalling the warp; the FP64 sum sees the same
-                    // terms in the same order
+                }
+            }
+        }
+        atomicAdd(&frc32[i].x, (float)((double)fx + cx));
+        atomicAdd(&frc32[i].y, (float)((double)fy + cy));
+        atomicAdd(&frc32[i].z, (float)((double)fz + cz));
+        if (THERMO) {
+            e += (double)ef;
+            w += (double)wf;
+            cnt = (double)ncnt;
+        }
+    }
+    if (THERMO) {
+        put_partial(part, 0, e, scratch);
+        put_partial(part, 1, w, scratch);
+        put_partial(part, 2, cnt, scratch);
+    }
+}
+
+// ---- mixed LJ, branch-free batches (full lists) --------------------------------
+// The pair arithmetic of k_lj_mixed_half, each pair seen from both atoms (no atomics),
+// arranged for instruction-level parallelism: the FP32 fast path of a batch's kB32 pairs runs without branches (the
+// force of a pair outside [close2, rc2_lo) is masked to zero), so the compiler
+// interleaves the pairs' dependent chains; the rare FP64-path pairs of a batch are
+// queued afterwards in list order.  The next batch's list entries are loaded before
+// the current batch's gathers, so a batch waits for one memory latency, not two.
+// The atom's FP64 position is re-read where it is needed (FP64 pairs, the epilogue)
+// instead of occupying registers through the loop.
+template <bool THERMO>
+__device__ __forceinline__ void fp64_lj_i(const double4* __restrict__ pos, int i, int j, const LjArgs& a, double& cx,
+                                          double& cy, double& cz, double& e, double& w, int& ncnt) {
+    fp64_lj<THERMO>(ldg_d4(pos + i), j, pos, a, cx, cy, cz, e, w, ncnt);
+}
+
+template <bool FUSE, bool THERMO, bool INIT = false>
+__global__ void __launch_bounds__(kThreads, TMD_MINB)
+k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
+              double4* __restrict__ vel, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
+              double* __restrict__ part, LjArgs a, double4* __restrict__ pos_n = nullptr,
+              float4* __restrict__ pos32_n = nullptr, const int* __restrict__ rbk = nullptr) {
+    __shared__ double scratch[kThreads / 32];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
+    prefetch_list_rows(nbl, n, a.stride, a.nbcap);
+    prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
+    prefetch_share(pos, (size_t)a.N * sizeof(double4));
+    if (FUSE) prefetch_share(vel, (size_t)a.N * sizeof(double4));
+    double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
+    if (i < a.N) {
+        const float4 ri = pos32[i];
+        float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
+        double cx = 0.0, cy = 0.0, cz = 0.0;
+        int ncnt = 0;
+        int nq = 0, q0 = 0, q1 = 0;  // deferred FP64 pairs
+        const uint32_t* lp = nbl + i;
+        const uint32_t pad = ((uint32_t)i << kCodeBits) | 21u;  // the atom itself, masked below
+        uint32_t ent[kB32];
+#pragma unroll
+        for (int u = 0; u < kB32; ++u) ent[u] = u < n ? __ldg(lp + (size_t)u * a.stride) : pad;
+        for (int k0 = 0; k0 < n; k0 += kB32) {
+            float4 rj[kB32];
+#pragma unroll
+            for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (ent[u] >> kCodeBits));
+            uint32_t cur[kB32];
+#pragma unroll
+            for (int u = 0; u < kB32; ++u) cur[u] = ent[u];
+#pragma unroll
+            for (int u = 0; u < kB32; ++u) {
+                const int q = k0 + kB32 + u;
+                ent[u] = q < n ? __ldg(lp + (size_t)q * a.stride) : pad;
+            }
+            unsigned slow = 0;
+#pragma unroll
+            for (int u = 0; u < kB32; ++u) {
+                const uint32_t en = cur[u];
+                const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
+                const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
+                const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
+                const float dx = fmaf(a.hx, sx, ri.x - rj[u].x);
+                const float dy = fmaf(a.hy, sy, ri.y - rj[u].y);
+                const float dz = fmaf(a.hz, sz, ri.z - rj[u].z);
+                const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool fast = rsq < a.rc2_lo && rsq >= a.close2;
+                // padding (the atom itself: rsq = 0) is neither fast nor queued
+                slow |= (!fast && rsq < a.rc2_hi && k0 + u < n) ? (1u << u) : 0u;
+                float sr2;
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
+                const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
+                float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
+                f = fast ? f : 0.f;
+                fx = fmaf(dx, f, fx);
+                fy = fmaf(dy, f, fy);
+                fz = fmaf(dz, f, fz);
+                if (THERMO) {
+                    ef += fast ? a.eps4f * sr6 * (sr6 - 1.0f) : 0.f;
+                    wf = fmaf(f, rsq, wf);
+                    ncnt += fast ? 1 : 0;
+                }
+            }
+            if (slow) {
+#pragma unroll
+                for (int u = 0; u < kB32; ++u) {
+                    if (!((slow >> u) & 1u)) continue;
+                    const int j = (int)(cur[u] >> kCodeBits);
                     if (nq == 2) {
-                        fp64_lj<THERMO>(pi, q0, pos, a, cx, cy, cz, e, w, ncnt);
-                        fp64_lj<THERMO>(pi, q1, pos, a, cx, cy, cz, e, w, ncnt);
+                        fp64_lj_i<THERMO>(pos, i, q0, a, cx, cy, cz, e, w, ncnt);
+                        fp64_lj_i<THERMO>(pos, i, q1, a, cx, cy, cz, e, w, ncnt);
                         nq = 0;
                     }
                     if (nq == 0) q0 = j;
@@ -326,32 +430,24 @@ k_lj_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, fl
                 }
             }
         }
-        if (!HALF) {
-            if (nq > 0) fp64_lj<THERMO>(pi, q0, pos, a, cx, cy, cz, e, w, ncnt);
-            if (nq > 1) fp64_lj<THERMO>(pi, q1, pos, a, cx, cy, cz, e, w, ncnt);
-        }
+        if (nq > 0) fp64_lj_i<THERMO>(pos, i, q0, a, cx, cy, cz, e, w, ncnt);
+        if (nq > 1) fp64_lj_i<THERMO>(pos, i, q1, a, cx, cy, cz, e, w, ncnt);
         const double Fx = (double)fx + cx, Fy = (double)fy + cy, Fz = (double)fz + cz;
-        if (HALF) {
-            atomicAdd(&frc32[i].x, (float)Fx);
-            atomicAdd(&frc32[i].y, (float)Fy);
-            atomicAdd(&frc32[i].z, (float)Fz);
-        } else {
-            const float4 F = make_float4((float)Fx, (float)Fy, (float)Fz, 0.f);
-            frc32[i] = F;
-            if (FUSE) {
-                double4 v = vel[i];
-                v.x += (double)F.x * a.h;
-                v.y += (double)F.y * a.h;
-                v.z += (double)F.z * a.h;
-                if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
-                if (INIT) {  // as k_integrate does it, from the FP32 force
-                    double4 x = integrate_one(pi, v, (double)F.x, (double)F.y, (double)F.z, a.dt_i, a.h_i);
-                    x.w = 0.0;  // positions carry w = 0
-                    pos_n[i] = x;
-                    pos32_n[i] = rebased32(x, rbk[i], a.alo, a.rb_h);
-                }
-                vel[i] = v;
+        const float4 F = make_float4((float)Fx, (float)Fy, (float)Fz, 0.f);
+        frc32[i] = F;
+        if (FUSE) {
+            double4 v = vel[i];
+            v.x += (double)F.x * a.h;
+            v.y += (double)F.y * a.h;
+            v.z += (double)F.z * a.h;
+            if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
+            if (INIT) {
+                double4 x = integrate_one(ldg_d4(pos + i), v, (double)F.x, (double)F.y, (double)F.z, a.dt_i, a.h_i);
+                x.w = 0.0;  // positions carry w = 0
+                pos_n[i] = x;
+                pos32_n[i] = rebased32(x, rbk[i], a.alo, a.rb_h);
             }
+            vel[i] = v;
         }
         if (THERMO) {
             e += (double)ef;
@@ -460,7 +556,7 @@ k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, dou
 struct DemMixedArgs {
     float rc2_lo, rc2_hi, c2_lo, c2_hi;  // margins around rc^2 and (2R)^2
     float d2, dn, dt_, k, mu;            // 2R and the model parameters
-    float hx, hy, hz;                    // rebasing shift decode scales (as k_lj_mixed)
+    float hx, hy, hz;                    // rebasing shift decode scales (as k_lj_mixed_bf)
 };
 
 template <bool HALF>
@@ -748,11 +844,15 @@ template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
 void launch_lj(State& s, const LjArgs& a, int nb) {
     double4* vel = s.vel.b[s.vc];
     double4* pn = INIT ? s.pos.b[1 - s.pc] : nullptr;
-    if (s.precision == 1)
-        k_lj_mixed<HALF, FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(
-            s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, vel, s.nbn, s.nbl, s.groot, s.red_part, a, pn,
-            INIT ? s.pos32.b[1 - s.pc] : nullptr, s.rbk);
-    else
+    if (s.precision == 1) {
+        if constexpr (HALF)
+            k_lj_mixed_half<THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, s.nbn,
+                                                                   s.nbl, s.groot, s.red_part, a);
+        else
+            k_lj_mixed_bf<FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(
+                s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, vel, s.nbn, s.nbl, s.red_part, a, pn,
+                INIT ? s.pos32.b[1 - s.pc] : nullptr, s.rbk);
+    } else
         k_lj_fp64<HALF, FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn,
                                                                           s.nbl, s.groot, s.red_part, a, pn);
 }

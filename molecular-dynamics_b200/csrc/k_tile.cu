@@ -26,8 +26,9 @@
 // k_lj_tile_mixed: stages the halo's rebased FP32 positions in shared memory
 // (16 bytes per atom, a plain copy: pos32.w carries the rebasing cell) and
 // runs the pair loop against it, reading two bytes of list per neighbour.
-// The pair arithmetic, the FP64 fallback and the summation order are those of
-// k_lj_mixed, so the forces are bit-identical to it.
+// The pair arithmetic and the FP64 fallback are those of the plain-list mixed
+// kernel (k_lj_mixed_bf); the summation order differs, so the forces agree with
+// it to FP32 rounding.
 
 #include <algorithm>
 #include <cmath>
@@ -361,9 +362,9 @@ k_build_tiles(const double4* __restrict__ pos, const int* __restrict__ rbk, cons
 // list pair the fields differ by dk in {-1, 0, 1} (the builder checks that no
 // field wraps), so w_j - w_i + 0x00100401 holds dk + 1 in bits 0-1 (x), 10-11
 // (y) and 20-21 (z) without borrows, and dk * (-rb_h) is built exactly as in
-// k_lj_mixed: an integer OR into the float 2^23, one subtraction, and a scale
+// k_lj_mixed_bf: an integer OR into the float 2^23, one subtraction, and a scale
 // (-rb_h, -rb_h / 2^10, -rb_h / 2^20: exact for rb_h a multiple of 1/8).  The
-// pair arithmetic and the FP64 fallback are k_lj_mixed's.
+// pair arithmetic and the FP64 fallback are k_lj_mixed_bf's.
 //
 // Work distribution: a warp walks its stream 32 consecutive positions at a
 // time (lane l takes position p0 + l), so every lane has a pair in every step
@@ -418,7 +419,7 @@ __device__ __forceinline__ void stream_step(int p0, int m, int lane, int warp, i
         const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
         if (rsq < a.rc2_hi) {
             if (rsq < a.rc2_lo && rsq >= a.close2) {
-                float sr2;  // hardware reciprocal, as in k_lj_mixed
+                float sr2;  // hardware reciprocal, as in k_lj_mixed_bf
                 asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
                 const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
                 const float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
