@@ -189,17 +189,19 @@ __global__ void k_root_list(const int* __restrict__ nbn, const uint32_t* __restr
     }
 }
 
-// loss pieces at x_T: MSD sum over locals, dU/dsigma sum, and the initial adjoint
-// a_x = (2/N)(x_T + img L - x_0) - F/N, a_v = dt a_x (drift of step T-1)
+// loss pieces at x_T: MSD sum over locals, dU/dsigma sum, the pair energy (FP64, each
+// pair seen from both atoms), and the initial adjoint a_x = (2/N)(x_T + img L - x_0) - F/N,
+// a_v = dt a_x (drift of step T-1).  The three sums are compensated, per block as (sum,
+// correction) rows of part: the loss enters central differences of ~1e-12.
 __global__ void __launch_bounds__(kT)
 k_adj_init(const double4* __restrict__ pos, const int* __restrict__ img, const int* __restrict__ ref,
            const double4* __restrict__ x0, const double4* __restrict__ frc, const float4* __restrict__ frc32,
            int mixed, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, double4* __restrict__ ax,
            double4* __restrict__ av, double* __restrict__ part, int N, int stride, int nbcap, double rc2,
            double sigma6, double eps, double inv_sigma, double len0, double len1, double len2, double dt) {
-    __shared__ double scratch[kT / 32];
+    __shared__ double scratch[64];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double msd = 0.0, dus = 0.0;
+    double msd = 0.0, dus = 0.0, ue = 0.0, dus_c = 0.0, ue_c = 0.0, np_ = 0.0, np_c = 0.0;
     if (i < N) {
         const double4 p = pos[i];
         const int im = img[i];
@@ -228,15 +230,39 @@ k_adj_init(const double4* __restrict__ pos, const int* __restrict__ img, const i
             if (s < rc2) {
                 const double sr2 = 1.0 / s;
                 const double sr6 = sr2 * sr2 * sr2 * sigma6;
-                dus += 12.0 * eps * inv_sigma * (2.0 * sr6 * sr6 - sr6);  // full list: 1/2 of 24 eps/sigma (...)
+                // full list: 1/2 of 24 eps/sigma (...) and 1/2 of the pair energy
+                dd_add(dus, dus_c, 12.0 * eps * inv_sigma * (2.0 * sr6 * sr6 - sr6), 0.0);
+                dd_add(ue, ue_c, 2.0 * eps * sr6 * (sr6 - 1.0), 0.0);
+                np_ += 0.5;  // pairs inside the cutoff (exact: halves of small integers)
             }
         }
     }
-    const double a1 = block_sum(msd, scratch);
-    const double a2 = block_sum(dus, scratch);
+    double msd_c = 0.0;
+    block_sum_dd(msd, msd_c, scratch);
+    block_sum_dd(dus, dus_c, scratch);
+    block_sum_dd(ue, ue_c, scratch);
+    block_sum_dd(np_, np_c, scratch);
     if (threadIdx.x == 0) {
-        part[blockIdx.x] = a1;
-        part[gridDim.x + blockIdx.x] = a2;
+        const int nb = gridDim.x;
+        part[blockIdx.x] = msd;
+        part[nb + blockIdx.x] = msd_c;
+        part[2 * nb + blockIdx.x] = dus;
+        part[3 * nb + blockIdx.x] = dus_c;
+        part[4 * nb + blockIdx.x] = ue;
+        part[5 * nb + blockIdx.x] = ue_c;
+        part[6 * nb + blockIdx.x] = np_;
+        part[7 * nb + blockIdx.x] = np_c;
+    }
+}
+
+// out[q] = the compensated total of rows (2q, 2q + 1) of part[.][nb]
+__global__ void k_sum_rows_dd(const double* __restrict__ part, double* __restrict__ out, int nb, int nq) {
+    __shared__ double scratch[64];
+    for (int q = 0; q < nq; ++q) {
+        double s = 0.0, c = 0.0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) dd_add(s, c, part[2 * q * nb + b], part[(2 * q + 1) * nb + b]);
+        block_sum_dd(s, c, scratch);
+        if (threadIdx.x == 0) out[q] = s + c;
     }
 }
 
@@ -433,11 +459,9 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     rebuild(s);
     run_force_lj(s, force_params(), false, 0.0);
     for (int t = 0; t < cfg.steps; ++t) {
-        if (t + 1 == cfg.steps) s.thermo = 1;  // U(x_T) for the loss
         forward_step(s, t, true);
         if ((t + 1) % cfg.reneigh == 0 && t + 1 < cfg.steps) checkpoint(s, (t + 1) / cfg.reneigh);
     }
-    s.thermo = 0;
     cudaEventRecord(e1, s.stream);
     // loss: MSD and U at x_T, and the initial adjoint state
     const int nb = nblk(N);
@@ -454,30 +478,28 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     dalloc(&gacc, 2 * (size_t)nbs + 2);
     dfree(&red);
     dalloc(&red, 8);
-    ensure_red_scratch(s, 2 * nb);
+    ensure_red_scratch(s, 8 * nb);
     const double sig6 = std::pow(sigma, 6);
     k_adj_init<<<nb, kT, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.ref.b[s.ac], x0_dev, s.frc.b[s.ac], s.frc32,
                                        s.precision, s.nbn, s.nbl, ax, av[0], s.red_part, N, s.nb_stride, s.nb_cap,
                                        cfg.cutoff * cfg.cutoff, sig6, epsilon, 1.0 / sigma, s.geo.len[0],
                                        s.geo.len[1], s.geo.len[2], cfg.dt);
     launched(K_ADJ_STEP);
-    k_sum_rows<<<1, 256, 0, s.stream>>>(s.red_part, red, nb, 2);
+    k_sum_rows_dd<<<1, 256, 0, s.stream>>>(s.red_part, red, nb, 4);
     launched(K_ADJ_STEP);
-    double sums[2] = {0, 0}, th[4] = {0, 0, 0, 0};
+    double sums[4] = {0, 0, 0, 0};
     TMD_CUDA(cudaMemcpyAsync(sums, red, sizeof(sums), cudaMemcpyDeviceToHost, s.stream));
-    TMD_CUDA(cudaMemcpyAsync(th, s.thermo_dev, sizeof(th), cudaMemcpyDeviceToHost, s.stream));
     TMD_CUDA(cudaStreamSynchronize(s.stream));
     float fms = 0.f;
     cudaEventElapsedTime(&fms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     run.fwd_ms = fms;
-    run.U = 0.5 * th[0];
+    run.U = sums[2];  // FP64 pair energy of x_T (for both forward precisions), compensated
     double dUds = sums[1];
     if (cfg.shifted) {
         // U_s = U - (pairs inside the cutoff) * e_c, e_c = 4 eps ((sigma/rc)^12 - (sigma/rc)^6);
-        // th[2] counts list entries inside the cutoff (each pair twice)
-        const double pairs = 0.5 * th[2];
+        const double pairs = sums[3];
         const double src6 = sig6 / std::pow(cfg.cutoff, 6);
         const double ec = 4.0 * epsilon * (src6 * src6 - src6);
         const double dec_ds = 4.0 * epsilon * (12.0 * src6 * src6 - 6.0 * src6) / sigma;

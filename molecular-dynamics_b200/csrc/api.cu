@@ -217,6 +217,11 @@ void free_all(State& s) {
                   &s.nbn, &s.scan_part, &s.slot_cell, &s.tile_desc, &s.tile_rows};
     for (int** q : ip) dfree(q);
     dfree(&s.frc32);
+    dfree(&s.img_cnt);
+    dfree(&s.img_slot);
+    dfree(&s.chain);
+    s.img_ok = 0;
+    s.ghosts_pushed = 0;
     dfree(&s.bmask);
     dfree(&s.nbl);
     dfree(&s.tile_stream);
@@ -236,7 +241,9 @@ void free_all(State& s) {
 // grows every per-slot array to hold `need` slots, keeping contents
 void grow_atoms(State& s, int need) {
     const int oldc = s.capA;
-    const int newc = need + need / 10 + 1024;
+    // a multiple of 64 slots: per-slot planes laid out back to back (img_slot) start on
+    // 256-byte boundaries, as bulk prefetches need
+    const int newc = (need + need / 10 + 1024 + 63) & ~63;
     const size_t o = (size_t)oldc, n = (size_t)newc;
     for (int b = 0; b < 2; ++b) {
         realloc_keep(&s.pos.b[b], o, n, s.stream);
@@ -256,6 +263,13 @@ void grow_atoms(State& s, int need) {
         dfree(q);
         dalloc(q, n);
     }
+    dfree(&s.img_cnt);
+    dalloc(&s.img_cnt, 2 * n);
+    dfree(&s.img_slot);
+    dalloc(&s.img_slot, (size_t)kImgW * n);
+    dfree(&s.chain);
+    dalloc(&s.chain, n);
+    s.img_ok = 0;
     s.capA = newc;
     if (oldc > 0) std::printf("0> reallocate_particle_capacity(): %d\n", newc);
 }
@@ -664,9 +678,10 @@ void md_synchronize_ghost_layer(void) {
     flush_final(s);
     flush_force(s);
     phase_mark(PH_COMM);
-    if (s.pend_ghost) {
+    if (s.pend_ghost) {  // the fused kernel wrote the locals, and the ghosts if it could
         s.pend_ghost = false;
-        run_ghost_refresh(s, s.ghost_exact ? 2 : 1);
+        const int gm = s.ghost_exact ? 2 : 1;
+        if (s.ghosts_pushed != gm) run_ghost_refresh(s, gm);
     } else if (s.pend_init) {
         s.pend_init = false;
         run_integrate(s, s.pend_dt, true);

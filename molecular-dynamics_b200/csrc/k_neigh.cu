@@ -324,6 +324,31 @@ __global__ void k_ghost_links(const int* __restrict__ ref, const int* __restrict
     rref[N + h] = broot_ref[g];
 }
 
+// ghost images by local, for the force kernel that also integrates: a local's direct
+// two-phase images (ghosts whose source it is) and all its images (ghosts whose root it is),
+// one plane per image number (planes filled in order, -1 beyond the last); ghosts whose
+// two-phase source is another ghost go to `chain`.  The order within a local's record follows
+// the atomics, but every ghost is written exactly once, so the result is deterministic.
+__global__ void k_image_map(const int* __restrict__ gsrc, const int* __restrict__ groot, int* __restrict__ img_cnt,
+                            int* __restrict__ img_slot, int* __restrict__ chain, DevStatus* st, int N, int G,
+                            int capA) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= G) return;
+    const int t = N + h;
+    const int s1 = gsrc[h];
+    if (s1 < N) {
+        const int k = atomicAdd(&img_cnt[s1], 1);
+        if (k < kImg1) img_slot[(size_t)k * capA + s1] = t;
+        else atomicAdd(&st->img_over1, 1);
+    } else {
+        chain[atomicAdd(&st->nchain, 1)] = h;
+    }
+    const int r = groot[h];
+    const int k2 = atomicAdd(&img_cnt[capA + r], 1);
+    if (k2 < kImg2) img_slot[(size_t)(kImg1 + k2) * capA + r] = t;
+    else atomicAdd(&st->img_over2, 1);
+}
+
 // ---- neighbour lists ---------------------------------------------------------
 // rebasing cell k relative to b, 8 bits per axis with bias 128 (|k - b| < 128 per axis
 // for atoms a few cells apart); differences of two such values carry no borrow while
@@ -670,11 +695,20 @@ void run_distribute(State& s) {
     s.pc = np;
     s.vc = nv;
     s.ac = na;
+    TMD_CUDA(cudaMemsetAsync(&s.status_dev->nchain, 0, 3 * sizeof(int), s.stream));  // with img_over1, 2
     if (s.G > 0) {
         k_ghost_links<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.slot_of_ref, s.bsrc_ref, s.broot_ref,
                                                                s.bcode, s.gsrc, s.groot, s.gcode, s.rref, N, s.G);
         launched(K_BIN);
+        TMD_CUDA(cudaMemsetAsync(s.img_cnt, 0, sizeof(int) * N, s.stream));
+        TMD_CUDA(cudaMemsetAsync(s.img_cnt + s.capA, 0, sizeof(int) * N, s.stream));
+        TMD_CUDA(cudaMemsetAsync(s.img_slot, 0xff, sizeof(int) * kImgW * (size_t)s.capA, s.stream));
+        k_image_map<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.gsrc, s.groot, s.img_cnt, s.img_slot, s.chain,
+                                                             s.status_dev, N, s.G, s.capA);
+        launched(K_BIN);
     }
+    s.img_ok = 0;  // known after the status readback of the list build
+    s.nchain = 0;
     prof_end(K_BIN);
     s.lists_valid = 0;
     s.tiles_valid = 0;
@@ -754,6 +788,8 @@ int run_build_lists(State& s, bool half, double cutoff) {
         }
         if (s.status_host->bad_code > 0 && s.precision == 1)
             set_error(3, "list pair spans more than one rebasing cell; mixed forces are invalid");
+        s.nchain = s.status_host->nchain;
+        s.img_ok = (s.status_host->img_over1 == 0 ? 1 : 0) | (s.status_host->img_over2 == 0 ? 2 : 0);
         const int mx = s.status_host->max_nb;
         if (mx <= s.nb_cap) {
             s.lists_valid = 1;

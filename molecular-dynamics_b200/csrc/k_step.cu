@@ -21,8 +21,11 @@ namespace tmd {
 
 namespace {
 
+// 128-thread blocks: 1,024 blocks for 131k atoms spread evenly over 148 SMs (6-7 each);
+// 256-thread blocks left 68 SMs with four and 80 with three, and ran 5 % (mixed) to 11 %
+// (FP64) slower in the force kernels
 #ifndef TMD_THREADS
-#define TMD_THREADS 256
+#define TMD_THREADS 128
 #endif
 constexpr int kThreads = TMD_THREADS;
 constexpr int kThermoQ = 4;  // partials: energy, virial, pairs inside the cutoff, v.v
@@ -111,19 +114,89 @@ __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, d
 constexpr int kB64 = TMD_B64;  // neighbours loaded per batch (FP64)
 constexpr int kB32 = TMD_B32;  // neighbours loaded per batch (mixed)
 
+// Ghost images written by the force kernel that integrates (maps from k_image_map): each
+// local writes the ghosts that are its images, from its new position, and extra threads
+// write the two-phase ghosts whose source is another ghost, from that source's previous
+// value.  The arithmetic is k_ghost_refresh's, so the ghosts are bit-identical to it.
+struct PushArgs {
+    const int* slot = nullptr;   // first image plane of the ghost mode (planes `plane` apart)
+    const int* chain = nullptr;  // two-phase ghosts whose source is a ghost
+    const int* gsrc = nullptr;
+    const int* gcode = nullptr;
+    const int* rbk = nullptr;
+    int nchain = 0;              // two-phase mode only
+    int base = 0;                // shift field of the code: 0 last pass, 8 total
+    int planes = 0;              // image planes of the mode
+    int plane = 0;               // plane stride (slot capacity)
+    int G = 0;
+    double len[3] = {0.0, 0.0, 0.0};
+};
+
+template <bool MIXED>
+__device__ __forceinline__ void write_ghost(int t, const double4& xs, int code, const PushArgs& pa,
+                                            double4* __restrict__ pos_n, float4* __restrict__ pos32_n,
+                                            const double* alo, double rb_h) {
+    double4 x;
+    x.x = dadd(xs.x, dmul(pa.len[0], (double)shift_axis(code, pa.base, 0)));
+    x.y = dadd(xs.y, dmul(pa.len[1], (double)shift_axis(code, pa.base, 1)));
+    x.z = dadd(xs.z, dmul(pa.len[2], (double)shift_axis(code, pa.base, 2)));
+    x.w = 0.0;
+    pos_n[t] = x;
+    if (MIXED) pos32_n[t] = rebased32(x, pa.rbk[t], alo, rb_h);
+}
+
+// the first three planes are read together (a local near one face, edge or corner of the box
+// has one, two or three two-phase images); further ones, for thin boxes, one by one
+template <bool MIXED>
+__device__ __forceinline__ void push_images(int i, const double4& x, int N, const PushArgs& pa,
+                                            double4* __restrict__ pos_n, float4* __restrict__ pos32_n,
+                                            const double* alo, double rb_h) {
+    int t[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) t[k] = pa.slot[(size_t)k * pa.plane + i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (t[k] < 0) return;
+        write_ghost<MIXED>(t[k], x, pa.gcode[t[k] - N], pa, pos_n, pos32_n, alo, rb_h);
+    }
+    for (int k = 3; k < pa.planes; ++k) {
+        const int tk = pa.slot[(size_t)k * pa.plane + i];
+        if (tk < 0) return;
+        write_ghost<MIXED>(tk, x, pa.gcode[tk - N], pa, pos_n, pos32_n, alo, rb_h);
+    }
+}
+
+// L2 prefetch of what the pushes read: the first image planes, ghost codes, rebasing cells
+__device__ __forceinline__ void prefetch_push(const PushArgs& pa, int N) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) prefetch_share(pa.slot + (size_t)k * pa.plane, (size_t)((N + 3) & ~3) * sizeof(int));
+    prefetch_share(pa.gcode, (size_t)((pa.G + 3) & ~3) * sizeof(int));
+    prefetch_share(pa.rbk, (size_t)((N + pa.G + 3) & ~3) * sizeof(int));
+}
+
+template <bool MIXED>
+__device__ __forceinline__ void push_chain(int q, const double4* __restrict__ pos_o, int N, const PushArgs& pa,
+                                           double4* __restrict__ pos_n, float4* __restrict__ pos32_n,
+                                           const double* alo, double rb_h) {
+    const int h = pa.chain[q];
+    write_ghost<MIXED>(N + h, pos_o[pa.gsrc[h]], pa.gcode[h], pa, pos_n, pos32_n, alo, rb_h);
+}
+
 // INIT (with FUSE, full lists): the epilogue also does the next step's initial integration
 // and writes the atom's new position to pos_n, the other buffer (neighbours read pos)
-template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
+// PUSH (with INIT): the kernel also writes the ghosts (PushArgs)
+template <bool HALF, bool FUSE, bool THERMO, bool INIT = false, bool PUSH = false>
 __global__ void __launch_bounds__(kThreads)
 k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* __restrict__ vel,
           const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot,
-          double* __restrict__ part, LjArgs a, double4* __restrict__ pos_n = nullptr) {
+          double* __restrict__ part, LjArgs a, double4* __restrict__ pos_n = nullptr, PushArgs pa = PushArgs()) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_list_rows(nbl, n, a.stride, a.nbcap);
     prefetch_share(pos, (size_t)a.NA * sizeof(double4));
     if (FUSE) prefetch_share(vel, (size_t)a.N * sizeof(double4));
+    if (PUSH) prefetch_push(pa, a.N);
     double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
     if (i < a.N) {
         const double4 pi = pos[i];
@@ -189,10 +262,13 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
                     double4 x = integrate_one(pi, v, fx, fy, fz, a.dt_i, a.h_i);
                     x.w = 0.0;
                     pos_n[i] = x;
+                    if (PUSH) push_images<false>(i, x, a.N, pa, pos_n, nullptr, a.alo, a.rb_h);
                 }
                 vel[i] = v;
             }
         }
+    } else if (PUSH && i < a.N + pa.nchain) {
+        push_chain<false>(i - a.N, pos, a.N, pa, pos_n, nullptr, a.alo, a.rb_h);
     }
     if (THERMO) {
         put_partial(part, 0, e, scratch);
@@ -349,12 +425,13 @@ __device__ __forceinline__ void fp64_lj_i(const double4* __restrict__ pos, int i
     fp64_lj<THERMO>(ldg_d4(pos + i), j, pos, a, cx, cy, cz, e, w, ncnt);
 }
 
-template <bool FUSE, bool THERMO, bool INIT = false>
+template <bool FUSE, bool THERMO, bool INIT = false, bool PUSH = false>
 __global__ void __launch_bounds__(kThreads, TMD_MINB)
 k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
               double4* __restrict__ vel, const int* __restrict__ nbn, const uint32_t* __restrict__ nbl,
               double* __restrict__ part, LjArgs a, double4* __restrict__ pos_n = nullptr,
-              float4* __restrict__ pos32_n = nullptr, const int* __restrict__ rbk = nullptr) {
+              float4* __restrict__ pos32_n = nullptr, const int* __restrict__ rbk = nullptr,
+              PushArgs pa = PushArgs()) {
     __shared__ double scratch[kThreads / 32];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
@@ -362,6 +439,8 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
     prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
     prefetch_share(pos, (size_t)a.N * sizeof(double4));
     if (FUSE) prefetch_share(vel, (size_t)a.N * sizeof(double4));
+    if (INIT) prefetch_share(rbk, (size_t)((a.N + 3) & ~3) * sizeof(int));
+    if (PUSH) prefetch_push(pa, a.N);
     double e = 0.0, w = 0.0, cnt = 0.0, ke = 0.0;
     if (i < a.N) {
         const float4 ri = pos32[i];
@@ -446,6 +525,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
                 x.w = 0.0;  // positions carry w = 0
                 pos_n[i] = x;
                 pos32_n[i] = rebased32(x, rbk[i], a.alo, a.rb_h);
+                if (PUSH) push_images<true>(i, x, a.N, pa, pos_n, pos32_n, a.alo, a.rb_h);
             }
             vel[i] = v;
         }
@@ -454,6 +534,8 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
             w += (double)wf;
             cnt = (double)ncnt;
         }
+    } else if (PUSH && i < a.N + pa.nchain) {
+        push_chain<true>(i - a.N, pos, a.N, pa, pos_n, pos32_n, a.alo, a.rb_h);
     }
     if (THERMO) {
         put_partial(part, 0, e, scratch);
@@ -840,8 +922,8 @@ StepArgs step_args(const State& s, double dt) {
 }
 
 // INIT: the kernels write the integrated locals into the other position buffer
-template <bool HALF, bool FUSE, bool THERMO, bool INIT = false>
-void launch_lj(State& s, const LjArgs& a, int nb) {
+template <bool HALF, bool FUSE, bool THERMO, bool INIT = false, bool PUSH = false>
+void launch_lj(State& s, const LjArgs& a, int nb, const PushArgs& pa = PushArgs()) {
     double4* vel = s.vel.b[s.vc];
     double4* pn = INIT ? s.pos.b[1 - s.pc] : nullptr;
     if (s.precision == 1) {
@@ -849,12 +931,12 @@ void launch_lj(State& s, const LjArgs& a, int nb) {
             k_lj_mixed_half<THERMO><<<nb, kThreads, 0, s.stream>>>(s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, s.nbn,
                                                                    s.nbl, s.groot, s.red_part, a);
         else
-            k_lj_mixed_bf<FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(
+            k_lj_mixed_bf<FUSE, THERMO, INIT, PUSH><<<nb, kThreads, 0, s.stream>>>(
                 s.pos32.b[s.pc], s.pos.b[s.pc], s.frc32, vel, s.nbn, s.nbl, s.red_part, a, pn,
-                INIT ? s.pos32.b[1 - s.pc] : nullptr, s.rbk);
+                INIT ? s.pos32.b[1 - s.pc] : nullptr, s.rbk, pa);
     } else
-        k_lj_fp64<HALF, FUSE, THERMO, INIT><<<nb, kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn,
-                                                                          s.nbl, s.groot, s.red_part, a, pn);
+        k_lj_fp64<HALF, FUSE, THERMO, INIT, PUSH><<<nb, kThreads, 0, s.stream>>>(
+            s.pos.b[s.pc], s.frc.b[s.ac], vel, s.nbn, s.nbl, s.groot, s.red_part, a, pn, pa);
 }
 
 }  // namespace
@@ -941,15 +1023,38 @@ void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double 
     a.hz = (float)(-s.geo.rb_h / 16.0);
     a.dt_i = dt_init;
     a.h_i = 0.5 * dt_init;
-    const int nb = nblocks(N, kThreads);
+    // the ghosts of the current mode are written too when the image maps are complete
+    const int gm = s.ghost_exact ? 2 : 1;
+    const bool push = s.G > 0 && ((s.img_ok >> (gm - 1)) & 1);
+    PushArgs pa;
+    if (push) {
+        pa.slot = s.img_slot + (gm == 2 ? (size_t)kImg1 * s.capA : 0);
+        pa.planes = gm == 2 ? kImg2 : kImg1;
+        pa.plane = s.capA;
+        pa.G = s.G;
+        pa.chain = s.chain;
+        pa.gsrc = s.gsrc;
+        pa.gcode = s.gcode;
+        pa.rbk = s.rbk;
+        pa.nchain = gm == 1 ? s.nchain : 0;
+        pa.base = gm == 1 ? 0 : 8;
+        for (int d = 0; d < 3; ++d) pa.len[d] = s.geo.len[d];
+    }
+    const int nb = nblocks(N + pa.nchain, kThreads);
     const bool thermo = s.thermo != 0;
     if (thermo) ensure_red_scratch(s, kThermoQ * nb);
     prof_begin(K_FORCE_LJ);
-    if (thermo) launch_lj<false, true, true, true>(s, a, nb);
-    else launch_lj<false, true, false, true>(s, a, nb);
+    if (push) {
+        if (thermo) launch_lj<false, true, true, true, true>(s, a, nb, pa);
+        else launch_lj<false, true, false, true, true>(s, a, nb, pa);
+    } else {
+        if (thermo) launch_lj<false, true, true, true>(s, a, nb);
+        else launch_lj<false, true, false, true>(s, a, nb);
+    }
     launched(K_FORCE_LJ);
     prof_end(K_FORCE_LJ);
     s.pc = 1 - s.pc;  // the locals of the other buffer are current; its ghosts follow
+    s.ghosts_pushed = (push || s.G == 0) ? gm : 0;
     s.integration_iters = N;
     if (thermo) {
         k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 0, kThermoQ);

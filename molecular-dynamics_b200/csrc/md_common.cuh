@@ -57,6 +57,39 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     return v;
 }
+// compensated sums (Knuth's two-sum: a + b = s + e exactly), for totals whose
+// rounding must stay far below their differences (loss values under central differences)
+__device__ __forceinline__ void dd_add(double& s, double& c, double t, double d) {
+    const double u = s + t;
+    const double bp = u - s;
+    c = c + d + ((s - (u - bp)) + (t - bp));
+    s = u;
+}
+__device__ __forceinline__ void warp_sum_dd(double& s, double& c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t = __shfl_down_sync(0xffffffffu, s, o);
+        const double d = __shfl_down_sync(0xffffffffu, c, o);
+        dd_add(s, c, t, d);
+    }
+}
+// block total of (s, c) pairs in thread 0 (scratch: 64 doubles)
+__device__ __forceinline__ void block_sum_dd(double& s, double& c, double* scratch) {
+    warp_sum_dd(s, c);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) {
+        scratch[wid] = s;
+        scratch[32 + wid] = c;
+    }
+    __syncthreads();
+    const int nw = blockDim.x >> 5;
+    if (wid == 0) {
+        s = lane < nw ? scratch[lane] : 0.0;
+        c = lane < nw ? scratch[32 + lane] : 0.0;
+        warp_sum_dd(s, c);
+    }
+    __syncthreads();
+}
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(0xffffffffu, v, o));

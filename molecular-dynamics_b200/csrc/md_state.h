@@ -57,7 +57,17 @@ struct DevStatus {
     int tile_overflow;  // slot blocks the tiled builder could not take (halo or row limits)
     int halo_max;       // largest staged halo of the last tiled build
     int tile_blocks;    // row blocks of the last tiled build
+    int nchain;         // ghosts whose two-phase source is a ghost (last distribution)
+    int img_over1;      // locals with more than kImg1 direct images
+    int img_over2;      // locals with more than kImg2 images in all
 };
+
+// periodic images a local can push (two-phase: its own first-pass images, one per face
+// it is near; exact: all its images, up to seven where the box is wider than two
+// ghost layers; a local with more leaves the map incomplete and the ghosts to a kernel)
+constexpr int kImg1 = 6;
+constexpr int kImg2 = 8;
+constexpr int kImgW = kImg1 + kImg2;
 
 struct PendingForce {
     bool valid = false;
@@ -113,6 +123,15 @@ struct State {
     int* tmp_src = nullptr;    // per sorted position: old slot
     int* perm = nullptr;       // new slot -> old slot
     int* slot_cell = nullptr;  // per (sorted) slot: its cell, ncells when outside the grid
+    // ghost images by local (k_image_map at every distribution): the force kernel that does
+    // the next initial integration writes them, so no separate ghost refresh is needed
+    int* img_cnt = nullptr;    // [2][capA]: direct two-phase images of a local, all its images
+    int* img_slot = nullptr;   // [kImgW][capA]: their slots by plane (kImg1 two-phase planes, then
+                               // kImg2 exact ones), -1 after a local's last image
+    int* chain = nullptr;      // [capA]: ghost indices whose two-phase source is a ghost
+    int nchain = 0;            // their number (status readback of the list build)
+    int img_ok = 0;            // bit gm - 1: the map of ghost mode gm (1, 2) is complete
+    int ghosts_pushed = 0;     // ghost mode whose images the last fused kernel wrote (0: none)
     // border pass
     unsigned* bmask = nullptr;   // per local (reference order): 26-bit ghost-type mask
     int* bcount = nullptr;       // [26][nblk] counts, scanned in place
