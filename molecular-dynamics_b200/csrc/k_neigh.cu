@@ -3,8 +3,9 @@
 //   * ghost generation (borders)     (comm/comm.impala:105-127, 528-642, 723-734; comm/lb.impala:88-100)
 //   * cell binning as a counting sort that reorders the device arrays by cell
 //                                    (core/grid.impala:280-321, 406-426)
-//   * neighbour-list build, one warp per cell, ballot/popc compaction
-//                                    (core/neighborlist.impala:1-78)
+//   * neighbour-list build, one warp per cell, homes grouped by octant of the
+//     cell, candidates filtered by the octant's home bounding box, ballot/popc
+//     compaction                     (core/neighborlist.impala:1-78)
 //
 // Ghost order.  The reference runs six passes (x+, x-, y+, y-, z+, z-); a
 // pass scans locals then all earlier ghosts in order and appends the ones
@@ -388,6 +389,10 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
     __shared__ int s_hcnt[kNlWarps][kHomeMax];
     __shared__ int s_rstart[kNlWarps][54];
     __shared__ int s_rpre[kNlWarps][55];
+    __shared__ unsigned char s_oidx[kNlWarps][kTile];       // a tile's candidates kept for one octant
+    __shared__ float s_obox[kNlWarps][8][6];                // per octant: bounding box of its homes
+    __shared__ unsigned long long s_omask[kNlWarps][8];     // per octant: its homes (bits of the batch)
+    static_assert(kTile <= 256 && kHomeMax <= 64, "octant indices are bytes, home masks 64 bits");
 
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * kNlWarps + wid;
@@ -442,6 +447,46 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
             s_hcnt[wid][q] = 0;
         }
         __syncwarp();
+        {  // octant of each home (sign of its offset from the cell centre) and per-octant boxes
+            const bool v0 = lane < hn, v1 = lane + 32 < hn;
+            const float4 p0 = s_hpos[wid][v0 ? lane : 0], p1 = s_hpos[wid][v1 ? lane + 32 : 0];
+            const int o0 = (p0.x >= 0.f) | ((p0.y >= 0.f) << 1) | ((p0.z >= 0.f) << 2);
+            const int o1 = (p1.x >= 0.f) | ((p1.y >= 0.f) << 1) | ((p1.z >= 0.f) << 2);
+            for (int o = 0; o < 8; ++o) {
+                const bool in0 = v0 && o0 == o, in1 = v1 && o1 == o;
+                const unsigned m0 = __ballot_sync(0xffffffffu, in0), m1 = __ballot_sync(0xffffffffu, in1);
+                if ((m0 | m1) == 0u) {
+                    if (lane == 0) s_omask[wid][o] = 0ull;
+                    continue;
+                }
+                float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+                if (in0) {
+                    lo[0] = hi[0] = p0.x;
+                    lo[1] = hi[1] = p0.y;
+                    lo[2] = hi[2] = p0.z;
+                }
+                if (in1) {
+                    lo[0] = fminf(lo[0], p1.x), hi[0] = fmaxf(hi[0], p1.x);
+                    lo[1] = fminf(lo[1], p1.y), hi[1] = fmaxf(hi[1], p1.y);
+                    lo[2] = fminf(lo[2], p1.z), hi[2] = fmaxf(hi[2], p1.z);
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
+                        hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
+                    }
+                if (lane == 0) {
+                    s_omask[wid][o] = (unsigned long long)m0 | ((unsigned long long)m1 << 32);
+                    for (int d = 0; d < 3; ++d) {
+                        s_obox[wid][o][d] = lo[d];
+                        s_obox[wid][o][3 + d] = hi[d];
+                    }
+                }
+            }
+            __syncwarp();
+        }
         for (int t0 = 0; t0 < M; t0 += kTile) {
             const int tn = min(kTile, M - t0);
             for (int m = t0 + lane; m < t0 + tn; m += 32) {
@@ -459,52 +504,85 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 s_crbk[wid][m - t0] = rel_cell(rbk[slot], rb0);
             }
             __syncwarp();
-            for (int h = 0; h < hn; ++h) {
-                const int i = hb + h;
-                const float4 hp = s_hpos[wid][h];
-                const int iref = HM ? ref[i] : 0;
-                const int irel = rel_cell(rbk[i], rb0);
-                int cnt = s_hcnt[wid][h];
+            // Homes are grouped by octant of their cell; a candidate is tested against an
+            // octant's homes only if it lies within the list cutoff (with the FP32 margin) of
+            // their bounding box.  Kept candidates stay in stencil order, so each home's list
+            // is the per-candidate test's, entry for entry.
+            for (int o = 0; o < 8; ++o) {
+                unsigned long long hm = s_omask[wid][o];
+                if (hm == 0ull) continue;
+                const float bx0 = s_obox[wid][o][0], by0 = s_obox[wid][o][1], bz0 = s_obox[wid][o][2];
+                const float bx1 = s_obox[wid][o][3], by1 = s_obox[wid][o][4], bz1 = s_obox[wid][o][5];
+                int nco = 0;
                 for (int q0 = 0; q0 < tn; q0 += 32) {
                     const int q = q0 + lane;
-                    bool pred = false;
-                    int slot = -1;
-                    int code = 0;
+                    bool keep = false;
                     if (q < tn) {
                         const float4 cp = s_cpos[wid][q];
-                        slot = __float_as_int(cp.w);
-                        const float dx = hp.x - cp.x, dy = hp.y - cp.y, dz = hp.z - cp.z;
-                        const float r2 = dx * dx + dy * dy + dz * dz;
-                        bool in = r2 < a.lo2;
-                        if (!in && r2 <= a.hi2) {
-                            // near the cutoff: the reference's exact FP64 test
-                            const double4 pi = pos[i], pj = pos[slot];
-                            in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
-                        }
-                        // core/neighborlist.impala:34: half lists keep i > j (reference index);
-                        // HM == 2 compares ghosts by their root so pairs across the
-                        // periodic boundary are kept once
-                        pred = in && slot != i && (!HM || s_cref[wid][HM ? q : 0] < iref);
-                        if (pred) {
-                            // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow
-                            // shows up as bits above bit 1 or in byte 3) means |dk| > 1
-                            const uint32_t d = (uint32_t)(s_crbk[wid][q] - irel + 0x010101);
-                            if ((d & 0xFFFCFCFCu) || (d & (d >> 1) & 0x010101u)) {
-                                atomicAdd(&st->bad_code, 1);
-                                code = 21;  // dk = 0
-                            } else {
-                                code = (int)((d & 3u) | ((d >> 6) & 0xCu) | ((d >> 12) & 0x30u));
+                        const float ex = fmaxf(fmaxf(bx0 - cp.x, cp.x - bx1), 0.f);
+                        const float ey = fmaxf(fmaxf(by0 - cp.y, cp.y - by1), 0.f);
+                        const float ez = fmaxf(fmaxf(bz0 - cp.z, cp.z - bz1), 0.f);
+                        keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= a.hi2;
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                    if (keep) {
+                        const int at = nco + __popc(bal & lt);
+                        s_oidx[wid][at] = (unsigned char)q;
+                    }
+                    nco += __popc(bal);
+                }
+                __syncwarp();
+                while (hm) {
+                    const int h = __ffsll((long long)hm) - 1;
+                    hm &= hm - 1ull;
+                    const int i = hb + h;
+                    const float4 hp = s_hpos[wid][h];
+                    const int iref = HM ? ref[i] : 0;
+                    const int irel = rel_cell(rbk[i], rb0);
+                    int cnt = s_hcnt[wid][h];
+                    for (int q0 = 0; q0 < nco; q0 += 32) {
+                        const int qq = q0 + lane;
+                        bool pred = false;
+                        int slot = -1;
+                        int code = 0;
+                        if (qq < nco) {
+                            const int q = s_oidx[wid][qq];
+                            const float4 cp = s_cpos[wid][q];
+                            slot = __float_as_int(cp.w);
+                            const float dx = hp.x - cp.x, dy = hp.y - cp.y, dz = hp.z - cp.z;
+                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                            bool in = r2 < a.lo2;
+                            if (!in && r2 <= a.hi2) {
+                                // near the cutoff: the reference's exact FP64 test
+                                const double4 pi = pos[i], pj = pos[slot];
+                                in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
+                            }
+                            // core/neighborlist.impala:34: half lists keep i > j (reference index);
+                            // HM == 2 compares ghosts by their root so pairs across the periodic
+                            // boundary are kept once
+                            pred = in && slot != i && (!HM || s_cref[wid][HM ? q : 0] < iref);
+                            if (pred) {
+                                // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow
+                                // shows up as bits above bit 1 or in byte 3) means |dk| > 1
+                                const uint32_t d = (uint32_t)(s_crbk[wid][q] - irel + 0x010101);
+                                if ((d & 0xFFFCFCFCu) || (d & (d >> 1) & 0x010101u)) {
+                                    atomicAdd(&st->bad_code, 1);
+                                    code = 21;  // dk = 0
+                                } else {
+                                    code = (int)((d & 3u) | ((d >> 6) & 0xCu) | ((d >> 12) & 0x30u));
+                                }
                             }
                         }
+                        const unsigned bal = __ballot_sync(0xffffffffu, pred);
+                        if (pred) {
+                            const int p = cnt + __popc(bal & lt);
+                            if (p < a.nbcap) nbl[(size_t)p * a.stride + i] = ((uint32_t)slot << kCodeBits) | (uint32_t)code;
+                        }
+                        cnt += __popc(bal);
                     }
-                    const unsigned bal = __ballot_sync(0xffffffffu, pred);
-                    if (pred) {
-                        const int p = cnt + __popc(bal & lt);
-                        if (p < a.nbcap) nbl[(size_t)p * a.stride + i] = ((uint32_t)slot << kCodeBits) | (uint32_t)code;
-                    }
-                    cnt += __popc(bal);
+                    if (lane == 0) s_hcnt[wid][h] = cnt;
+                    __syncwarp();
                 }
-                if (lane == 0) s_hcnt[wid][h] = cnt;
                 __syncwarp();
             }
             __syncwarp();
