@@ -55,6 +55,7 @@ UNIT = "atom-steps/s"
 CELLS = (32, 32, 32)
 DT = 0.005
 L2_FLUSH_BYTES = 256 << 20
+PROFILE_EVERY = 10  # force launches timed by events: one in ten, spread over the timed steps
 DRIFT_STEPS = 1000
 DRIFT_EVERY = 50
 
@@ -249,6 +250,7 @@ def measure(lib, tm, parts, precision, steps, warmup, flush, half=False, force_f
     sim.run(dt, warmup)
     if profile_force:
         lib.md_profile_enable(1 << 0)
+        lib.md_profile_sample(PROFILE_EVERY)
         lib.md_profile_reset()
     step_ms = np.zeros(steps, dtype=np.float32)
     sim.run(dt, steps, step_ms=step_ms, flush=(ctypes.c_void_p(flush.data_ptr()), flush.numel() * 4))
@@ -257,6 +259,7 @@ def measure(lib, tm, parts, precision, steps, warmup, flush, half=False, force_f
         nl, t = ctypes.c_longlong(), ctypes.c_double()
         lib.md_profile_get(0, ctypes.byref(nl), ctypes.byref(t))
         lib.md_profile_enable(0)
+        lib.md_profile_sample(1)
         fms = t.value / max(nl.value, 1)
     sim.close()
     lib.md_set_half_mode(0)
@@ -356,7 +359,10 @@ def run_ours(args):
     lib.md_set_precision(1)
     sim = tm.Simulation(lib, *parts, temp=1.44)
     sim.run(DT, W)
-    lib.md_profile_enable(1 << 0)  # events around the LJ force launches
+    # events around one LJ force launch in PROFILE_EVERY (each pair of events costs the
+    # stream a few microseconds, so timing every launch would slow the timed steps)
+    lib.md_profile_enable(1 << 0)
+    lib.md_profile_sample(PROFILE_EVERY)
     lib.md_profile_reset()
     barrier(dist)
     with ClockSampler(local) as clk:
@@ -366,6 +372,7 @@ def run_ours(args):
     fms = ctypes.c_double()
     lib.md_profile_get(0, ctypes.byref(nl), ctypes.byref(fms))
     lib.md_profile_enable(0)
+    lib.md_profile_sample(1)
     # mean list length of the current lists (full list, FP64 cutoff 2.8)
     sizes = np.zeros(natoms, dtype=np.int32)
     lists = np.zeros((natoms, 1), dtype=np.int32)
@@ -439,7 +446,7 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
                      "bytes_per_atom": bytes_per_atom, "mean_list_length": mean_nb,
-                     "launch_ms": force_ms, "launches": nl.value,
+                     "launch_ms": force_ms, "launches_timed": nl.value, "timed_every": PROFILE_EVERY,
                      # list count and entries plus the atom's own FP64 position and force: what
                      # must come from HBM once per step whatever the gathers hit
                      "compulsory_bytes_per_atom": 4 + 4 * mean_nb + 48,

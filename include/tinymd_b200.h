@@ -192,10 +192,15 @@ void md_synchronize(void);
  * the library creates; NULL selects the legacy default stream. */
 void md_set_stream(void *stream);
 /* GPU time per timer bucket since md_initialize_grid, in ms:
- * out = {total, force, neigh, comm, balance, other} (main.cpp:477-484 buckets). */
+ * out = {total, force, neigh, comm, balance, other} (main.cpp:477-484 buckets).
+ * Zero unless md_set_phase_timing(1): the phase boundaries are CUDA events on the stream. */
 void md_get_phase_times(double *out);
+void md_set_phase_timing(int enable); /* default 0 */
 /* Kernel profiling with CUDA events on the library stream. */
 void md_profile_enable(int enable);
+/* Time one launch in `every` of each profiled kernel (default 1); md_profile_get then
+ * counts and sums the timed launches only.  Each timed launch adds two events to the stream. */
+void md_profile_sample(int every);
 int md_profile_count(void);
 const char *md_profile_name(int kernel_id);
 int md_profile_get(int kernel_id, long long *launches, double *total_ms);

@@ -83,6 +83,8 @@ std::deque<ProfRec> prof_q;
 long long prof_launch[K_COUNT] = {0};
 double prof_ms[K_COUNT] = {0};
 int prof_mask = 0;
+int prof_every = 1;
+long long prof_seen[K_COUNT] = {0};
 cudaEvent_t prof_open[K_COUNT] = {nullptr};
 
 cudaEvent_t get_event() {
@@ -128,8 +130,12 @@ void fold_prof(bool all) {
 }
 }  // namespace
 
+// device phase timing (md_get_phase_times) is opt-in: each mark is a timing event, and an
+// event on the stream costs a few microseconds of pipeline drain
+bool phase_on = false;
+
 void phase_mark(int phase) {
-    if (phase == cur_phase) return;
+    if (!phase_on || phase == cur_phase) return;
     cudaEvent_t e = get_event();
     TMD_CUDA(cudaEventRecord(e, g_state.stream));
     marks.push_back({e, phase});
@@ -138,9 +144,11 @@ void phase_mark(int phase) {
 }
 
 void phase_times(double* out6) {
-    cudaEvent_t e = get_event();
-    TMD_CUDA(cudaEventRecord(e, g_state.stream));
-    marks.push_back({e, cur_phase});
+    if (phase_on) {
+        cudaEvent_t e = get_event();
+        TMD_CUDA(cudaEventRecord(e, g_state.stream));
+        marks.push_back({e, cur_phase});
+    }
     fold_marks(true);
     double tot = 0;
     for (int p = 1; p < PH_COUNT; ++p) tot += phase_ms[p];
@@ -162,6 +170,7 @@ void phase_reset() {
 
 void prof_begin(int k) {
     if (!(prof_mask & (1 << k))) return;
+    if (prof_seen[k]++ % prof_every != 0) return;  // one launch in prof_every is timed
     prof_open[k] = get_event();
     TMD_CUDA(cudaEventRecord(prof_open[k], g_state.stream));
 }
@@ -180,6 +189,7 @@ void prof_reset() {
     for (int k = 0; k < K_COUNT; ++k) {
         prof_launch[k] = 0;
         prof_ms[k] = 0;
+        prof_seen[k] = 0;
     }
 }
 
@@ -677,15 +687,21 @@ void md_synchronize_ghost_layer(void) {
     if (!require_alive("md_synchronize_ghost_layer")) return;
     flush_final(s);
     flush_force(s);
-    phase_mark(PH_COMM);
+    // phase marks are timing events: set only where work is enqueued (an event on the
+    // stream costs a few microseconds of pipeline drain)
     if (s.pend_ghost) {  // the fused kernel wrote the locals, and the ghosts if it could
         s.pend_ghost = false;
         const int gm = s.ghost_exact ? 2 : 1;
-        if (s.ghosts_pushed != gm) run_ghost_refresh(s, gm);
+        if (s.ghosts_pushed != gm) {
+            phase_mark(PH_COMM);
+            run_ghost_refresh(s, gm);
+        }
     } else if (s.pend_init) {
         s.pend_init = false;
+        phase_mark(PH_COMM);
         run_integrate(s, s.pend_dt, true);
     } else {
+        phase_mark(PH_COMM);
         run_ghost_sync(s);
     }
 }
@@ -731,7 +747,6 @@ void md_final_integration(double dt) {
     flush_final(s);
     flush_ghost(s);
     flush_init(s);
-    phase_mark(PH_FORCE);
     if (s.pend_force.valid) {
         PendingForce p = s.pend_force;
         s.pend_force.valid = false;
@@ -744,12 +759,14 @@ void md_final_integration(double dt) {
             s.last_force_half = 0;
             return;
         }
+        phase_mark(PH_FORCE);
         if (!p.dem && !p.half) {
             launch_force(s, p, true, dt);
             return;
         }
         launch_force(s, p, false, 0.0);
     }
+    phase_mark(PH_FORCE);
     run_final(s, dt);
 }
 
@@ -1036,6 +1053,15 @@ void md_get_phase_times(double* out) {
 void md_profile_enable(int mask) {
     if (g_state.alive) flush_all(g_state);
     prof_mask = mask;
+}
+void md_set_phase_timing(int enable) {
+    if (g_state.alive) flush_all(g_state);
+    phase_on = enable != 0;
+    if (!phase_on) cur_phase = 0;
+}
+void md_profile_sample(int every) {
+    if (g_state.alive) flush_all(g_state);
+    prof_every = every > 0 ? every : 1;
 }
 int md_profile_count(void) { return K_COUNT; }
 const char* md_profile_name(int id) { return kernel_name(id); }

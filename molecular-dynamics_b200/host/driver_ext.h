@@ -35,6 +35,7 @@ inline void thermo(double* out) {
     out[2] = oracle_temperature() * (3.0 * n - 3.0);
 }
 inline bool phase_times(double*) { return false; }
+inline void enable_phase_timing() {}
 inline const char* backend() { return "cpu oracle (restatement of the reference cpu backend)"; }
 inline bool failed() { return false; }
 }  // namespace drv
@@ -58,6 +59,7 @@ inline bool phase_times(double* out6) {
     md_get_phase_times(out6);
     return true;
 }
+inline void enable_phase_timing() { md_set_phase_timing(1); }
 inline const char* backend() { return "B200 (sm_100a CUDA kernels)"; }
 inline bool failed() { return md_last_error() == MD_ERR_CUDA || md_last_error() == MD_ERR_NO_DEVICE; }
 }  // namespace drv

@@ -277,6 +277,7 @@ int main(int argc, char** argv) {
     md_get_node_bounding_box(world, &rank);
     const double volume = (world[1] - world[0]) * (world[3] - world[2]) * (world[5] - world[4]);
 
+    drv::enable_phase_timing();  // the time report's buckets come from the GPU timeline
     drv::set_precision(precision == "mixed" ? 1 : 0);
     drv::set_ghost_mode(ghost == "exact" ? 1 : 0);
     drv::set_half_mode(half_mode == "ghost" ? 1 : 0);

@@ -76,6 +76,8 @@ _EXTENSION_API = {
     "md_set_stream": (None, [_vp]),
     "md_get_phase_times": (None, [_vp]),
     "md_profile_enable": (None, [_c_int]),
+    "md_profile_sample": (None, [_c_int]),
+    "md_set_phase_timing": (None, [_c_int]),
     "md_profile_count": (_c_int, []),
     "md_profile_name": (ctypes.c_char_p, [_c_int]),
     "md_profile_get": (_c_int, [_c_int, ctypes.POINTER(_c_ll), ctypes.POINTER(_c_double)]),
