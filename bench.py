@@ -204,6 +204,16 @@ def run_reference(args):
     return 0
 
 
+def fused_kernel_bytes(mean_nb, ghosts_per_atom):
+    """Algorithmic bytes per atom of the timed force kernel, which also finishes the step and
+    starts the next one: the mixed full-list force (count, list entry and FP32 neighbour
+    position per pair, own position, FP32 force: 4 + 16 n + 24) and the integration with the
+    ghost update it took over (5 x 24 per atom, 4 + 3 + 24 + 24 per ghost)."""
+    force = 4 + mean_nb * (4 + 12) + 12 + 12
+    step = 5 * 24 + ghosts_per_atom * (4 + 3 + 24 + 24)
+    return force, step
+
+
 def timed_steps(lib, sim, steps, flush):
     """Device time of `steps` native timesteps, each bracketed by CUDA events on the
     library stream, with `flush` (a device buffer larger than L2) overwritten before
@@ -242,7 +252,8 @@ def energy_drift(lib, tm, parts, precision):
 
 def measure(lib, tm, parts, precision, steps, warmup, flush, half=False, force_field="lj", dem=(0.0, 0.0, 0.0, 0.0),
             cutoff=2.5, dt=DT, temp=1.44, profile_force=False):
-    """Device-timed steps of one workload in one form: (atom-steps/s, ms per step, force ms per launch or None)."""
+    """Device-timed steps of one workload in one form: (atom-steps/s, ms per step, None or, with
+    profile_force, (force ms per launch, ghosts per atom, mean list length))."""
     lib.md_set_precision(precision)
     if half:
         lib.md_set_half_mode(1)  # half lists that keep the periodic-boundary pairs
@@ -260,7 +271,11 @@ def measure(lib, tm, parts, precision, steps, warmup, flush, half=False, force_f
         lib.md_profile_get(0, ctypes.byref(nl), ctypes.byref(t))
         lib.md_profile_enable(0)
         lib.md_profile_sample(1)
-        fms = t.value / max(nl.value, 1)
+        natoms = len(parts[0])
+        sizes = np.zeros(natoms, dtype=np.int32)
+        lists = np.zeros((natoms, 1), dtype=np.int32)
+        lib.md_get_neighbor_lists(tm.ptr(sizes), tm.ptr(lists), 1)
+        fms = (t.value / max(nl.value, 1), sim.counts()[1] / natoms, float(sizes.mean()))
     sim.close()
     lib.md_set_half_mode(0)
     lib.md_set_precision(0)
@@ -284,11 +299,14 @@ def workloads(lib, tm, flush, peak):
     for name, prec in (("fp64", 0), ("mixed", 1)):
         row[name], _, fms[name] = measure(lib, tm, parts, prec, 500, 20, flush, profile_force=True)
     row["mixed_over_fp64"] = row["mixed"] / row["fp64"]
-    n = 75.0  # mean full-list length of the FCC liquid at this density (measured at 131k)
-    b32 = 4 + n * (4 + 12) + 12 + 12
-    achieved = len(parts[0]) * b32 / (fms["mixed"] * 1e-3) / 1e9
+    launch_ms, ghosts_per_atom, mean_nb = fms["mixed"]
+    fb, sb = fused_kernel_bytes(mean_nb, ghosts_per_atom)
+    b32 = fb + sb
+    achieved = len(parts[0]) * b32 / (launch_ms * 1e-3) / 1e9
     row["roofline_mixed_force"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                                   "frac": achieved / peak, "launch_ms": fms["mixed"], "bytes_per_atom": b32}
+                                   "frac": achieved / peak, "launch_ms": launch_ms, "bytes_per_atom": b32,
+                                   "force_bytes_per_atom": fb, "integrate_ghost_bytes_per_atom": sb,
+                                   "mean_list_length": mean_nb}
     out["lj_half_fcc_64x64x64_524288_atoms_full_list"] = row
     # DEM at 48^3: the FCC diagonal split and the reference's granular gas, with the
     # reference closure (zero force) and the contact-fixed model (R = 0.6)
@@ -378,6 +396,7 @@ def run_ours(args):
     lists = np.zeros((natoms, 1), dtype=np.int32)
     lib.md_get_neighbor_lists(tm.ptr(sizes), tm.ptr(lists), 1)
     mean_nb = float(sizes.mean())
+    ghosts_per_atom = sim.counts()[1] / natoms
     # force and potential-energy error of the mixed form on the same state: both forms'
     # forces (and thermo sums) on the positions the timed run ended with
     lib.md_set_thermo(1)
@@ -415,13 +434,19 @@ def run_ours(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         s = tm.Simulation(lib, m, x, v, world_box, rank_box, temp=1.44)
+        lib.md_synchronize()
+        ta = time.perf_counter()
         s.run(DT, K)
+        lib.md_synchronize()
+        tb = time.perf_counter()
         mm, xx, vv, ff = s.arrays()
         t1 = time.perf_counter()
         nghost = s.counts()[1]
         s.close()
-        e2e_runs.append(t1 - t0)
-    e2e_value, e2e_ms = replica_rate(natoms, world, K, min(e2e_runs) * 1e3, dist, dev)
+        # (total, set-up: grid, device allocation, upload, first lists and force; steps; copy back)
+        e2e_runs.append((t1 - t0, ta - t0, tb - ta, t1 - tb))
+    best = min(e2e_runs)
+    e2e_value, e2e_ms = replica_rate(natoms, world, K, best[0] * 1e3, dist, dev)
     lib.md_set_precision(0)
     h2d = natoms * (8 + 24 + 24)
     d2h = (natoms + nghost) * (32 * 3 + 16 + 8 + 4)  # md_copy_data_from_accelerator
@@ -430,7 +455,8 @@ def run_ours(args):
     force_ms = fms.value / max(nl.value, 1)
     # algorithmic bytes per atom and force launch (payload only, padding excluded): the list
     # count, per neighbour a 4-byte index and a 12-byte FP32 position, own FP32 position, FP32 force
-    bytes_per_atom = 4 + mean_nb * (4 + 12) + 12 + 12
+    force_bytes, step_bytes = fused_kernel_bytes(mean_nb, ghosts_per_atom)
+    bytes_per_atom = force_bytes + step_bytes
     achieved = natoms * bytes_per_atom / (force_ms * 1e-3) / 1e9
     traffic = measured_traffic()
     line = {
@@ -445,7 +471,8 @@ def run_ours(args):
                   "mixed_max_force_err_over_rms": ferr, "mixed_energy_err": eerr},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
-                     "bytes_per_atom": bytes_per_atom, "mean_list_length": mean_nb,
+                     "bytes_per_atom": bytes_per_atom, "force_bytes_per_atom": force_bytes,
+                     "integrate_ghost_bytes_per_atom": step_bytes, "mean_list_length": mean_nb,
                      "launch_ms": force_ms, "launches_timed": nl.value, "timed_every": PROFILE_EVERY,
                      # list count and entries plus the atom's own FP64 position and force: what
                      # must come from HBM once per step whatever the gathers hit
@@ -453,7 +480,8 @@ def run_ours(args):
                      "compulsory_frac": natoms * (4 + 4 * mean_nb + 48) / (force_ms * 1e-3) / 1e9 / peak},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
-                "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock"},
+                "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock",
+                "setup_ms": best[1] * 1e3, "steps_ms": best[2] * 1e3, "copy_back_ms": best[3] * 1e3},
         "drift": drift,
         "adjoint": adj,
         "workloads": more,

@@ -290,7 +290,8 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
                           const int* __restrict__ ref_o, int* __restrict__ ref_n, const int* __restrict__ img_o,
                           int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rref,
                           int* __restrict__ rbk, const int* __restrict__ bin_cell, int* __restrict__ slot_cell,
-                          float4* __restrict__ pos32, int NA, int N, GeoArgs a, int mixed) {
+                          float4* __restrict__ pos32, int* __restrict__ img_cnt, int* __restrict__ img_slot,
+                          int capA, int NA, int N, GeoArgs a, int mixed) {
     int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= NA) return;
     int o = perm[n];
@@ -305,6 +306,11 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
     if (n < N) {
         img_n[n] = img_o[o];
         rref[n] = r;
+        // empty image records for k_ghost_links to fill
+        img_cnt[n] = 0;
+        img_cnt[capA + n] = 0;
+#pragma unroll
+        for (int k = 0; k < kImgW; ++k) img_slot[(size_t)k * capA + n] = -1;
     }
     slot_of_ref[r] = n;
     int k = rebase_cell(p, a);
@@ -312,31 +318,28 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
     if (mixed) pos32[n] = rebased32(p, k, a.alo, a.rb_h);
 }
 
+// Per ghost: its source, root and shift code in slot terms, and its place in the image
+// records of the locals (k_permute emptied them): a local's direct two-phase images (ghosts
+// whose source it is) and all its images (ghosts whose root it is), one plane per image
+// number (filled in order, -1 beyond the last); ghosts whose two-phase source is another
+// ghost go to `chain`.  The order within a record follows the atomics, but every ghost is
+// written exactly once, so the result is deterministic.
 __global__ void k_ghost_links(const int* __restrict__ ref, const int* __restrict__ slot_of_ref,
                               const int* __restrict__ bsrc_ref, const int* __restrict__ broot_ref,
                               const int* __restrict__ bcode, int* __restrict__ gsrc, int* __restrict__ groot,
-                              int* __restrict__ gcode, int* __restrict__ rref, int N, int G) {
+                              int* __restrict__ gcode, int* __restrict__ rref, int* __restrict__ img_cnt,
+                              int* __restrict__ img_slot, int* __restrict__ chain, DevStatus* st, int N, int G,
+                              int capA) {
     int h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= G) return;
     int g = ref[N + h] - N;
-    gsrc[h] = slot_of_ref[bsrc_ref[g]];
-    groot[h] = slot_of_ref[broot_ref[g]];
+    const int s1 = slot_of_ref[bsrc_ref[g]];
+    const int r = slot_of_ref[broot_ref[g]];
+    gsrc[h] = s1;
+    groot[h] = r;
     gcode[h] = bcode[g];
     rref[N + h] = broot_ref[g];
-}
-
-// ghost images by local, for the force kernel that also integrates: a local's direct
-// two-phase images (ghosts whose source it is) and all its images (ghosts whose root it is),
-// one plane per image number (planes filled in order, -1 beyond the last); ghosts whose
-// two-phase source is another ghost go to `chain`.  The order within a local's record follows
-// the atomics, but every ghost is written exactly once, so the result is deterministic.
-__global__ void k_image_map(const int* __restrict__ gsrc, const int* __restrict__ groot, int* __restrict__ img_cnt,
-                            int* __restrict__ img_slot, int* __restrict__ chain, DevStatus* st, int N, int G,
-                            int capA) {
-    const int h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= G) return;
     const int t = N + h;
-    const int s1 = gsrc[h];
     if (s1 < N) {
         const int k = atomicAdd(&img_cnt[s1], 1);
         if (k < kImg1) img_slot[(size_t)k * capA + s1] = t;
@@ -344,7 +347,6 @@ __global__ void k_image_map(const int* __restrict__ gsrc, const int* __restrict_
     } else {
         chain[atomicAdd(&st->nchain, 1)] = h;
     }
-    const int r = groot[h];
     const int k2 = atomicAdd(&img_cnt[capA + r], 1);
     if (k2 < kImg2) img_slot[(size_t)(kImg1 + k2) * capA + r] = t;
     else atomicAdd(&st->img_over2, 1);
@@ -680,6 +682,36 @@ __global__ void k_scan_apply(const int* __restrict__ in, int* __restrict__ out, 
     if (blockIdx.x == nb - 1 && threadIdx.x == 0) out[n] = part[nb];
 }
 
+// Exclusive scan of up to kScanSingleMax values in one block: the values are staged in
+// shared memory by coalesced loads, each thread scans a run of consecutive values there,
+// the block scans the run totals, and the results leave by coalesced stores.  One launch
+// instead of three for the counts of a rebuild (tens of thousands of values).
+constexpr int kScanSingleMax = 32768;  // 128 KiB of shared memory
+__global__ void __launch_bounds__(kScanThreads) k_scan_single(const int* __restrict__ in, int* __restrict__ out,
+                                                               int n) {
+    extern __shared__ int sv[];
+    __shared__ int sh[32];
+#pragma unroll 8
+    for (int k = threadIdx.x; k < n; k += kScanThreads) sv[k] = in[k];
+    __syncthreads();
+    const int run = (n + kScanThreads - 1) / kScanThreads;
+    const int base = threadIdx.x * run;
+    const int end = min(base + run, n);
+    int s = 0;
+    for (int k = base; k < end; ++k) s += sv[k];
+    int tot;
+    int ex = block_exscan(s, &tot, sh);
+    for (int k = base; k < end; ++k) {
+        const int v = sv[k];
+        sv[k] = ex;
+        ex += v;
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int k = threadIdx.x; k < n; k += kScanThreads) out[k] = sv[k];
+    if (threadIdx.x == 0) out[n] = tot;
+}
+
 // ---- host wrappers ---------------------------------------------------------------
 static inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
 
@@ -694,6 +726,17 @@ void ensure_scan_scratch(State& s, int n) {
 
 // out[0..n-1] = exclusive prefix sums of in, out[n] = total (in != out allowed only)
 void exclusive_scan(State& s, const int* in, int* out, int n) {
+    if (n <= kScanSingleMax) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            TMD_CUDA(cudaFuncSetAttribute(k_scan_single, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kScanSingleMax * (int)sizeof(int)));
+            attr_set = true;
+        }
+        k_scan_single<<<1, kScanThreads, (size_t)n * sizeof(int), s.stream>>>(in, out, n);
+        launched(K_SCAN);
+        return;
+    }
     int nb = nblocks(n, kScanBlock);
     if (nb < 1) nb = 1;
     ensure_scan_scratch(s, n);
@@ -753,7 +796,7 @@ void run_distribute(State& s) {
     if (NA == 0) return;
     prof_begin(K_BIN);
     TMD_CUDA(cudaMemsetAsync(s.cnt, 0, sizeof(int) * nseg, s.stream));
-    TMD_CUDA(cudaMemsetAsync(&s.status_dev->out_local, 0, 2 * sizeof(int), s.stream));
+    TMD_CUDA(cudaMemsetAsync(&s.status_dev->out_local, 0, 5 * sizeof(int), s.stream));  // .. img_over2
     k_bin_count<<<nblocks(NA, 256), 256, 0, s.stream>>>(s.pos.b[s.pc], s.cnt, s.bin_cell, s.bin_rank, s.status_dev,
                                                         N, NA, a);
     launched(K_BIN);
@@ -767,22 +810,16 @@ void run_distribute(State& s) {
     const int np = 1 - s.pc, nv = 1 - s.vc, na = 1 - s.ac;
     k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
         s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
-        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk, s.bin_cell, s.slot_cell, s.pos32.b[np], NA, N, a,
-        s.precision);
+        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk,
+        s.bin_cell, s.slot_cell, s.pos32.b[np], s.img_cnt, s.img_slot, s.capA, NA, N, a, s.precision);
     launched(K_BIN);
     s.pc = np;
     s.vc = nv;
     s.ac = na;
-    TMD_CUDA(cudaMemsetAsync(&s.status_dev->nchain, 0, 3 * sizeof(int), s.stream));  // with img_over1, 2
     if (s.G > 0) {
         k_ghost_links<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.slot_of_ref, s.bsrc_ref, s.broot_ref,
-                                                               s.bcode, s.gsrc, s.groot, s.gcode, s.rref, N, s.G);
-        launched(K_BIN);
-        TMD_CUDA(cudaMemsetAsync(s.img_cnt, 0, sizeof(int) * N, s.stream));
-        TMD_CUDA(cudaMemsetAsync(s.img_cnt + s.capA, 0, sizeof(int) * N, s.stream));
-        TMD_CUDA(cudaMemsetAsync(s.img_slot, 0xff, sizeof(int) * kImgW * (size_t)s.capA, s.stream));
-        k_image_map<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.gsrc, s.groot, s.img_cnt, s.img_slot, s.chain,
-                                                             s.status_dev, N, s.G, s.capA);
+                                                               s.bcode, s.gsrc, s.groot, s.gcode, s.rref, s.img_cnt,
+                                                               s.img_slot, s.chain, s.status_dev, N, s.G, s.capA);
         launched(K_BIN);
     }
     s.img_ok = 0;  // known after the status readback of the list build
@@ -820,9 +857,7 @@ int run_build_lists(State& s, bool half, double cutoff) {
         a.nxy = g.nx * g.ny;
         for (int d = 0; d < 3; ++d) a.alo[d] = g.aabb_lo[d];
         a.spacing = g.spacing;
-        TMD_CUDA(cudaMemsetAsync(&s.status_dev->max_nb, 0, sizeof(int), s.stream));
-        // bad_code, tile_overflow, halo_max and tile_blocks are adjacent
-        TMD_CUDA(cudaMemsetAsync(&s.status_dev->bad_code, 0, 4 * sizeof(int), s.stream));
+        TMD_CUDA(cudaMemsetAsync(&s.status_dev->max_nb, 0, 5 * sizeof(int), s.stream));  // .. tile_blocks
         prof_begin(K_NLIST);
         const int nb = nblocks(g.ncells, kNlWarps);
         // the tiled builder declines when its shared-memory need (halo capacity and

@@ -114,7 +114,7 @@ __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, d
 constexpr int kB64 = TMD_B64;  // neighbours loaded per batch (FP64)
 constexpr int kB32 = TMD_B32;  // neighbours loaded per batch (mixed)
 
-// Ghost images written by the force kernel that integrates (maps from k_image_map): each
+// Ghost images written by the force kernel that integrates (maps from k_ghost_links): each
 // local writes the ghosts that are its images, from its new position, and extra threads
 // write the two-phase ghosts whose source is another ghost, from that source's previous
 // value.  The arithmetic is k_ghost_refresh's, so the ghosts are bit-identical to it.

@@ -50,16 +50,18 @@ struct Geometry {
 // Device-side status words written by kernels and read back with one copy.
 struct DevStatus {
     int nghost;         // ghosts produced by the last border pass
-    int max_nb;         // longest neighbour list of the last build
+    // zeroed together before a binning (one memset): out_local .. img_over2
     int out_local;      // locals outside the cell grid at the last binning
     int out_ghost;      // ghosts outside the cell grid
+    int nchain;         // ghosts whose two-phase source is a ghost (last distribution)
+    int img_over1;      // locals with more than kImg1 direct images
+    int img_over2;      // locals with more than kImg2 images in all
+    // zeroed together before a list build (one memset): max_nb .. tile_blocks
+    int max_nb;         // longest neighbour list of the last build
     int bad_code;       // list pairs whose rebasing offset exceeded one cell
     int tile_overflow;  // slot blocks the tiled builder could not take (halo or row limits)
     int halo_max;       // largest staged halo of the last tiled build
     int tile_blocks;    // row blocks of the last tiled build
-    int nchain;         // ghosts whose two-phase source is a ghost (last distribution)
-    int img_over1;      // locals with more than kImg1 direct images
-    int img_over2;      // locals with more than kImg2 images in all
 };
 
 // periodic images a local can push (two-phase: its own first-pass images, one per face
@@ -123,7 +125,7 @@ struct State {
     int* tmp_src = nullptr;    // per sorted position: old slot
     int* perm = nullptr;       // new slot -> old slot
     int* slot_cell = nullptr;  // per (sorted) slot: its cell, ncells when outside the grid
-    // ghost images by local (k_image_map at every distribution): the force kernel that does
+    // ghost images by local (k_ghost_links at every distribution): the force kernel that does
     // the next initial integration writes them, so no separate ghost refresh is needed
     int* img_cnt = nullptr;    // [2][capA]: direct two-phase images of a local, all its images
     int* img_slot = nullptr;   // [kImgW][capA]: their slots by plane (kImg1 two-phase planes, then
