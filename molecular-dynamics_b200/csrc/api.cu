@@ -8,6 +8,7 @@
 //   md_compute_lennard_jones (full list) + md_final_integration -> one kernel
 // Every call that exposes data to the host drains pending work first.
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -227,6 +228,8 @@ void free_all(State& s) {
                   &s.nbn, &s.scan_part, &s.slot_cell, &s.tile_desc, &s.tile_rows};
     for (int** q : ip) dfree(q);
     dfree(&s.frc32);
+    dfree(&s.dl_buf);
+    s.dl_cap = 0;
     dfree(&s.img_cnt);
     dfree(&s.img_slot);
     dfree(&s.chain);
@@ -386,6 +389,46 @@ void* stage(size_t bytes) {
         if (!TMD_CUDA(cudaMallocHost(&stage_ptr, stage_bytes))) stage_bytes = 0;
     }
     return stage_ptr;
+}
+
+// device state -> the host mirror's layout, by reference index r (a permutation of the slots):
+// out = mass[NA], pos[NA][3], vel[NA][3], frc[NA][3]; ghost velocities only for the
+// contact-fixed DEM model, ghost forces zero (what md_copy_data_from_accelerator reports)
+__global__ void k_gather_ref(const double4* __restrict__ pos, const double4* __restrict__ vel,
+                             const double4* __restrict__ frc, const float4* __restrict__ frc32,
+                             const double* __restrict__ mass, const int* __restrict__ ref, double* __restrict__ out,
+                             int N, int NA, int mixed, int ghost_vel) {
+    const int slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= NA) return;
+    const int r = ref[slot];
+    if (r < 0 || r >= NA) return;
+    double* om = out;
+    double* op = out + NA;
+    double* ov = out + 4 * (size_t)NA;
+    double* of = out + 7 * (size_t)NA;
+    om[r] = mass[slot];
+    const double4 p = pos[slot];
+    op[3 * (size_t)r] = p.x;
+    op[3 * (size_t)r + 1] = p.y;
+    op[3 * (size_t)r + 2] = p.z;
+    double4 v = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (r < N || ghost_vel) v = vel[slot];
+    ov[3 * (size_t)r] = v.x;
+    ov[3 * (size_t)r + 1] = v.y;
+    ov[3 * (size_t)r + 2] = v.z;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    if (r < N) {
+        if (mixed) {
+            const float4 f = frc32[slot];
+            fx = f.x, fy = f.y, fz = f.z;
+        } else {
+            const double4 f = frc[slot];
+            fx = f.x, fy = f.y, fz = f.z;
+        }
+    }
+    of[3 * (size_t)r] = fx;
+    of[3 * (size_t)r + 1] = fy;
+    of[3 * (size_t)r + 2] = fz;
 }
 
 __global__ void k_iota(int* a, int* b, int* img, int n) {
@@ -597,37 +640,33 @@ void md_copy_data_to_accelerator(void) {
 void md_copy_data_from_accelerator(void) {
     State& s = g_state;
     if (!require_alive("md_copy_data_from_accelerator")) return;
-    Snapshot sn;
-    snapshot(s, sn);
+    flush_all(s);
     const int NA = s.N + s.G;
-    s.h_mass.assign(NA, 0.0);
-    s.h_pos.assign((size_t)NA * 3, 0.0);
-    s.h_vel.assign((size_t)NA * 3, 0.0);
-    s.h_frc.assign((size_t)NA * 3, 0.0);
-    for (int slot = 0; slot < NA; ++slot) {
-        const int r = sn.ref[slot];
-        if (r < 0 || r >= NA) continue;
-        s.h_mass[r] = sn.mass[slot];
-        s.h_pos[3 * r] = sn.pos[slot].x;
-        s.h_pos[3 * r + 1] = sn.pos[slot].y;
-        s.h_pos[3 * r + 2] = sn.pos[slot].z;
-        if (r < s.N || s.dem_fixed) {
-            s.h_vel[3 * r] = sn.vel[slot].x;
-            s.h_vel[3 * r + 1] = sn.vel[slot].y;
-            s.h_vel[3 * r + 2] = sn.vel[slot].z;
-        }
-        if (r < s.N) {
-            if (s.precision == 1) {
-                s.h_frc[3 * r] = sn.frc32[slot].x;
-                s.h_frc[3 * r + 1] = sn.frc32[slot].y;
-                s.h_frc[3 * r + 2] = sn.frc32[slot].z;
-            } else {
-                s.h_frc[3 * r] = sn.frc[slot].x;
-                s.h_frc[3 * r + 1] = sn.frc[slot].y;
-                s.h_frc[3 * r + 2] = sn.frc[slot].z;
-            }
-        }
+    // every element is overwritten below (the gather covers all NA reference indices)
+    s.h_mass.resize(NA);
+    s.h_pos.resize((size_t)NA * 3);
+    s.h_vel.resize((size_t)NA * 3);
+    s.h_frc.resize((size_t)NA * 3);
+    if (NA == 0) return;
+    // gathered into reference order on the device, one copy into pinned memory
+    const size_t words = (size_t)10 * NA;
+    if (words > s.dl_cap) {
+        dfree(&s.dl_buf);
+        s.dl_cap = words + words / 8 + 1024;
+        dalloc(&s.dl_buf, s.dl_cap);
     }
+    double* host = (double*)stage(sizeof(double) * words);
+    if (!host) return;
+    k_gather_ref<<<(NA + 255) / 256, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.frc32,
+                                                         s.mass.b[s.ac], s.ref.b[s.ac], s.dl_buf, s.N, NA,
+                                                         s.precision == 1, s.dem_fixed);
+    launched(K_MISC);
+    TMD_CUDA(cudaMemcpyAsync(host, s.dl_buf, sizeof(double) * words, cudaMemcpyDeviceToHost, s.stream));
+    sync_stream(s);
+    std::copy(host, host + NA, s.h_mass.begin());
+    std::copy(host + NA, host + 4 * (size_t)NA, s.h_pos.begin());
+    std::copy(host + 4 * (size_t)NA, host + 7 * (size_t)NA, s.h_vel.begin());
+    std::copy(host + 7 * (size_t)NA, host + 10 * (size_t)NA, s.h_frc.begin());
 }
 
 void md_exchange_particles(void) {  // comm/comm.impala:392-525: no remote ranks in one process

@@ -774,15 +774,28 @@ void run_borders(State& s) {
     // boff = exclusive scan of bcount, stored after the counts
     int* boff = s.bcount + n;
     exclusive_scan(s, s.bcount, boff, n);
+    // The ghost count comes back while the emit kernel already runs: emit writes only the
+    // slots below the capacity, so when the count shows the capacity was short the host
+    // grows the arrays (which waits for that emit) and emits again.  The host thus enqueues
+    // the next kernels before emit finishes instead of leaving the GPU idle for a round trip.
+    static cudaEvent_t counted = nullptr;
+    if (!counted) TMD_CUDA(cudaEventCreateWithFlags(&counted, cudaEventDisableTiming));
     TMD_CUDA(cudaMemcpyAsync(&s.status_host->nghost, boff + n, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    TMD_CUDA(cudaEventRecord(counted, s.stream));
+    auto emit = [&]() {
+        k_border_emit<<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
+                                                  s.ref.b[s.ac], s.slot_of_ref, s.bmask, boff, s.gsrc, s.groot,
+                                                  s.gcode, s.bsrc_ref, s.broot_ref, s.bcode, N, nblk, s.capA,
+                                                  a, s.dem_fixed);
+        launched(K_BORDER);
+    };
+    emit();
+    TMD_CUDA(cudaEventSynchronize(counted));
     const int G = s.status_host->nghost;
-    if (N + G > s.capA) grow_atoms(s, N + G);
-    k_border_emit<<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
-                                              s.ref.b[s.ac], s.slot_of_ref, s.bmask, boff, s.gsrc, s.groot,
-                                              s.gcode, s.bsrc_ref, s.broot_ref, s.bcode, N, nblk, s.capA,
-                                              a, s.dem_fixed);
-    launched(K_BORDER);
+    if (N + G > s.capA) {
+        grow_atoms(s, N + G);
+        emit();
+    }
     prof_end(K_BORDER);
     s.G = G;
     s.lists_valid = 0;

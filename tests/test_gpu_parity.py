@@ -68,8 +68,10 @@ def test_trajectory_bitwise_fp64_full(product, oracle):
         # the host-mirror path of the reference interface agrees too
         mp, xp2, vp2, fp2 = p.arrays()
         mo, xo2, vo2, fo2 = o.arrays()
+        np.testing.assert_array_equal(mp, mo)
         np.testing.assert_array_equal(xp2, xo2)
         np.testing.assert_array_equal(vp2, vo2)
+        np.testing.assert_array_equal(fp2, fo2)
         gp, go = p.ghost_arrays(), o.ghost_arrays()
         np.testing.assert_array_equal(gp[1], go[1])
     finally:
