@@ -127,6 +127,7 @@ struct State {
     int* slot_cell = nullptr;  // per (sorted) slot: its cell, ncells when outside the grid
     // ghost images by local (k_ghost_links at every distribution): the force kernel that does
     // the next initial integration writes them, so no separate ghost refresh is needed
+    char* slab = nullptr;      // the one allocation the per-slot arrays are carved from (grow_atoms)
     double* dl_buf = nullptr;  // md_copy_data_from_accelerator's gather (mass, pos, vel, frc by reference)
     size_t dl_cap = 0;         // its capacity in doubles
     int* img_cnt = nullptr;    // [2][capA]: direct two-phase images of a local, all its images
