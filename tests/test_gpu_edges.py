@@ -49,6 +49,14 @@ def test_ghost_capacity_growth(product, oracle):
     run_both(product, oracle, 40, cells=(2, 2, 2))
 
 
+@pytest.mark.parametrize("bench,cells", [("body_collision", (6, 6, 6)), ("half", (10, 10, 10))])
+def test_sparse_setups(product, oracle, bench, cells):
+    """The md driver's sparse setups, 40 steps bit-identical: body_collision (two bodies in a
+    world box extended by 20, mostly empty cells: initialize.h:297-362) and half (the lower half
+    of the box in y filled)."""
+    run_both(product, oracle, 40, benchmark=bench, cells=cells)
+
+
 def test_atom_outside_the_grid(product, oracle):
     """One atom starts 5 length units beyond the upper x face (outside the box extended by one
     2.8 cell): it is in no cell and no list; its ghost image (shifted by -L) lies inside and is
