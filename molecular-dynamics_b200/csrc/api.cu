@@ -344,11 +344,25 @@ void launch_force(State& s, const PendingForce& p, bool fuse_final, double dt) {
     else run_force_lj(s, p, fuse_final, dt);
 }
 
+// the held-back final kick joins the integration when one is pending (same arithmetic)
+double take_kick(State& s) {
+    if (!s.pend_kick) return -1.0;
+    s.pend_kick = false;
+    return s.pend_kick_dt;
+}
+
 void flush_init(State& s) {
     if (!s.pend_init) return;
     s.pend_init = false;
     phase_mark(PH_FORCE);
-    run_integrate(s, s.pend_dt, false);
+    run_integrate(s, s.pend_dt, false, take_kick(s));
+}
+
+void flush_kick(State& s) {
+    if (!s.pend_kick) return;
+    s.pend_kick = false;
+    phase_mark(PH_FORCE);
+    run_final(s, s.pend_kick_dt);
 }
 
 void flush_force(State& s) {
@@ -380,6 +394,7 @@ void flush_all(State& s) {
     flush_final(s);
     flush_ghost(s);
     flush_init(s);
+    flush_kick(s);
     flush_force(s);
 }
 
@@ -572,7 +587,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.lists_valid = 0;
     s.pend_init = false;
     s.pend_force = PendingForce();
-    s.pend_final = s.pend_ghost = false;
+    s.pend_final = s.pend_ghost = s.pend_kick = false;
     s.force_iters = s.rsq_iters = s.integration_iters = 0;
     s.launches = 0;
     allocate_state(s, n, neighborlist_capacity);
@@ -723,6 +738,11 @@ void md_initial_integration(double dt) {
         s.pend_ghost = true;
         return;
     }
+    if (s.pend_kick && !s.pend_final && !s.pend_ghost && !s.pend_init && !s.pend_force.valid) {
+        s.pend_init = true;  // the held-back kick stays pending and joins this integration
+        s.pend_dt = dt;
+        return;
+    }
     flush_all(s);
     s.pend_init = true;
     s.pend_dt = dt;
@@ -732,6 +752,7 @@ void md_synchronize_ghost_layer(void) {
     State& s = g_state;
     if (!require_alive("md_synchronize_ghost_layer")) return;
     flush_final(s);
+    if (!s.pend_init) flush_kick(s);
     flush_force(s);
     // phase marks are timing events: set only where work is enqueued (an event on the
     // stream costs a few microseconds of pipeline drain)
@@ -745,7 +766,7 @@ void md_synchronize_ghost_layer(void) {
     } else if (s.pend_init) {
         s.pend_init = false;
         phase_mark(PH_COMM);
-        run_integrate(s, s.pend_dt, true);
+        run_integrate(s, s.pend_dt, true, take_kick(s));
     } else {
         phase_mark(PH_COMM);
         run_ghost_sync(s);
@@ -793,6 +814,7 @@ void md_final_integration(double dt) {
     flush_final(s);
     flush_ghost(s);
     flush_init(s);
+    flush_kick(s);
     if (s.pend_force.valid) {
         PendingForce p = s.pend_force;
         s.pend_force.valid = false;
@@ -811,6 +833,13 @@ void md_final_integration(double dt) {
             return;
         }
         launch_force(s, p, false, 0.0);
+        if (!s.thermo) {
+            // held back: the next initial integration applies it first (one launch fewer); the
+            // thermo sums take their kinetic energy from the separate kick, so not with thermo
+            s.pend_kick = true;
+            s.pend_kick_dt = dt;
+            return;
+        }
     }
     phase_mark(PH_FORCE);
     run_final(s, dt);

@@ -36,6 +36,8 @@ struct StepArgs {
     int N, G, stride;
     double dt, h;  // h = 0.5 * dt as the reference computes it
     double len[3], alo[3], rb_h;
+    int pre;       // k_integrate first applies the previous step's final kick v += hp f
+    double hp;
 };
 
 struct DemArgs {
@@ -87,6 +89,12 @@ __device__ __forceinline__ void prefetch_share(const void* base, size_t bytes) {
         const unsigned len = (unsigned)min((size_t)4096, hi - o);
         asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"((const char*)base + o), "r"(len) : "memory");
     }
+}
+
+// one vector atomic (sm_90+: red.global.add.v4.f32) instead of three scalar ones for a
+// half-list reaction on an FP32 force; w stays zero
+__device__ __forceinline__ void add_force32(float4* f, float x, float y, float z) {
+    atomicAdd(f, make_float4(x, y, z, 0.f));
 }
 
 // target of the reaction force of a half-list pair: the local itself or a ghost's root
@@ -362,9 +370,7 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
                     fx += px;
                     fy += py;
                     fz += pz;
-                    atomicAdd(&frc32[t].x, -px);
-                    atomicAdd(&frc32[t].y, -py);
-                    atomicAdd(&frc32[t].z, -pz);
+                    add_force32(frc32 + t, -px, -py, -pz);
                     if (THERMO) {
                         ef += a.eps4f * sr6 * (sr6 - 1.0f);
                         wf += f * rsq;
@@ -382,9 +388,7 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
                         cx += ex * f;
                         cy += ey * f;
                         cz += ez * f;
-                        atomicAdd(&frc32[t].x, (float)(-ex * f));
-                        atomicAdd(&frc32[t].y, (float)(-ey * f));
-                        atomicAdd(&frc32[t].z, (float)(-ez * f));
+                        add_force32(frc32 + t, (float)(-ex * f), (float)(-ey * f), (float)(-ez * f));
                         if (THERMO) {
                             e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
                             w += f * r2;
@@ -394,9 +398,7 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
                 }
             }
         }
-        atomicAdd(&frc32[i].x, (float)((double)fx + cx));
-        atomicAdd(&frc32[i].y, (float)((double)fy + cy));
-        atomicAdd(&frc32[i].z, (float)((double)fz + cz));
+        add_force32(frc32 + i, (float)((double)fx + cx), (float)((double)fy + cy), (float)((double)fz + cz));
         if (THERMO) {
             e += (double)ef;
             w += (double)wf;
@@ -680,9 +682,7 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
                     cz += o[2];
                     if (HALF) {
                         const int t = reaction_slot(j, a.N, groot);
-                        atomicAdd(&frc32[t].x, (float)(-o[0]));
-                        atomicAdd(&frc32[t].y, (float)(-o[1]));
-                        atomicAdd(&frc32[t].z, (float)(-o[2]));
+                        add_force32(frc32 + t, (float)(-o[0]), (float)(-o[1]), (float)(-o[2]));
                     }
                 }
                 continue;
@@ -710,17 +710,13 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
             fz += pz;
             if (HALF) {
                 const int t = reaction_slot(j, a.N, groot);
-                atomicAdd(&frc32[t].x, -px);
-                atomicAdd(&frc32[t].y, -py);
-                atomicAdd(&frc32[t].z, -pz);
+                add_force32(frc32 + t, -px, -py, -pz);
             }
         }
     }
     const float Fx = (float)((double)fx + cx), Fy = (float)((double)fy + cy), Fz = (float)((double)fz + cz);
     if (HALF) {
-        atomicAdd(&frc32[i].x, Fx);
-        atomicAdd(&frc32[i].y, Fy);
-        atomicAdd(&frc32[i].z, Fz);
+        add_force32(frc32 + i, Fx, Fy, Fz);
     } else {
         frc32[i] = make_float4(Fx, Fy, Fz, 0.f);
     }
@@ -733,6 +729,13 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
 //         ghost source still holds the previous step's value (so chained
 //         edge / corner ghosts lag, exactly like comm/comm.impala:334-388);
 //     2 = exact periodic images: ghost = integrated root + total shift.
+
+// v += h f in the reference's operand order (core/compute.impala:186-194), as k_final does it
+__device__ __forceinline__ void kick(double4& v, double fx, double fy, double fz, double h) {
+    v.x = dadd(v.x, dmul(fx, h));
+    v.y = dadd(v.y, dmul(fy, h));
+    v.z = dadd(v.z, dmul(fz, h));
+}
 
 template <bool MIXED>
 __device__ __forceinline__ void load_force(const double4* frc, const float4* frc32, int i, double& fx, double& fy,
@@ -757,6 +760,7 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
         double4 v = vel_o[t];
         double fx, fy, fz;
         load_force<MIXED>(frc, frc32, t, fx, fy, fz);
+        if (a.pre) kick(v, fx, fy, fz, a.hp);
         const double4 x = integrate_one(pos_o[t], v, fx, fy, fz, a.dt, a.h);
         pos_n[t] = x;
         vel_n[t] = v;
@@ -778,6 +782,7 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
         double4 vs = vel_o[s];
         double fx, fy, fz;
         load_force<MIXED>(frc, frc32, s, fx, fy, fz);
+        if (a.pre) kick(vs, fx, fy, fz, a.hp);
         xs = integrate_one(pos_o[s], vs, fx, fy, fz, a.dt, a.h);
     } else {
         xs = pos_o[s];
@@ -795,9 +800,8 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
         double4 vr = vel_o[r];
         double fx, fy, fz;
         load_force<MIXED>(frc, frc32, r, fx, fy, fz);
-        vr.x = dadd(vr.x, dmul(fx, a.h));
-        vr.y = dadd(vr.y, dmul(fy, a.h));
-        vr.z = dadd(vr.z, dmul(fz, a.h));
+        if (a.pre) kick(vr, fx, fy, fz, a.hp);
+        kick(vr, fx, fy, fz, a.h);
         vel_n[t] = vr;
     }
 }
@@ -918,6 +922,8 @@ StepArgs step_args(const State& s, double dt) {
         a.alo[d] = s.geo.aabb_lo[d];
     }
     a.rb_h = s.geo.rb_h;
+    a.pre = 0;
+    a.hp = 0.0;
     return a;
 }
 
@@ -1141,10 +1147,14 @@ void run_force_dem(State& s, const PendingForce& p) {
     prof_end(K_FORCE_DEM);
 }
 
-void run_integrate(State& s, double dt, bool fuse_ghosts) {
+void run_integrate(State& s, double dt, bool fuse_ghosts, double kick_dt) {
     const int NA = s.N + s.G;
     if (NA == 0) return;
     StepArgs a = step_args(s, dt);
+    if (kick_dt >= 0.0) {  // the previous step's final kick first (k_final's arithmetic)
+        a.pre = 1;
+        a.hp = 0.5 * kick_dt;
+    }
     const int gm = fuse_ghosts ? (s.ghost_exact ? 2 : 1) : 0;
     const bool mixed = s.precision == 1;
     const bool demv = s.dem_fixed != 0;

@@ -179,6 +179,9 @@ struct State {
     // call is known, fused with the next step's initial integration when that is the call
     bool pend_final = false;
     double pend_final_dt = 0.0;
+    // the final kick of a half-list or DEM force, held back to join the next initial integration
+    bool pend_kick = false;
+    double pend_kick_dt = 0.0;
     PendingForce final_cfg;
     // locals were integrated by that fused kernel; ghosts still to be refreshed or carried
     bool pend_ghost = false;
@@ -225,7 +228,9 @@ bool tile_cap_fits(const State& s, int cap);  // the tiled builder can stage hal
 void run_force_lj_tiles(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_dem(State& s, const PendingForce& p);
-void run_integrate(State& s, double dt, bool fuse_ghosts);
+// kick_dt >= 0: the previous step's final kick of kick_dt is applied first (held back by
+// md_final_integration for forces whose kernel cannot take it)
+void run_integrate(State& s, double dt, bool fuse_ghosts, double kick_dt = -1.0);
 void run_ghost_sync(State& s);
 void run_final(State& s, double dt);
 void run_refresh_pos32(State& s);
