@@ -31,7 +31,7 @@
 
 namespace tmd {
 
-void grow_atoms(State& s, int need);
+bool grow_atoms(State& s, int need);
 
 namespace {
 

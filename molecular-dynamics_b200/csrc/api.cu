@@ -262,8 +262,9 @@ void free_all(State& s) {
 
 }  // namespace
 
-// grows every per-slot array to hold `need` slots, keeping contents
-void grow_atoms(State& s, int need) {
+// grows every per-slot array to hold `need` slots, keeping contents; false (error latched,
+// arrays unchanged) when the device has no room
+bool grow_atoms(State& s, int need) {
     const int oldc = s.capA;
     // a multiple of 64 slots: per-slot planes laid out back to back (img_slot) start on
     // 256-byte boundaries, as bulk prefetches need
@@ -274,7 +275,7 @@ void grow_atoms(State& s, int need) {
     for (const SlabItem& it : items) total += (it.elem * it.elems * n + 255) & ~(size_t)255;
     char* slab = nullptr;
     dalloc(&slab, total);
-    if (!slab) return;
+    if (!slab) return false;
     size_t off = 0;
     for (SlabItem& it : items) {
         char* q = slab + off;
@@ -292,6 +293,7 @@ void grow_atoms(State& s, int need) {
     s.img_ok = 0;
     s.capA = newc;
     if (oldc > 0) std::printf("0> reallocate_particle_capacity(): %d\n", newc);
+    return true;
 }
 
 void grow_lists(State& s, int rows) {
@@ -304,9 +306,9 @@ void grow_lists(State& s, int rows) {
 
 namespace {
 
-void allocate_state(State& s, int N, int nb_cap) {
+bool allocate_state(State& s, int N, int nb_cap) {
     s.capA = 0;
-    grow_atoms(s, N + N / 2 + 64);
+    if (!grow_atoms(s, N + N / 2 + 64)) return false;
     const int ncells = s.geo.ncells;
     const int nseg = 2 * (ncells + 1);
     dalloc(&s.cnt, nseg + 1);
@@ -325,6 +327,7 @@ void allocate_state(State& s, int N, int nb_cap) {
     TMD_CUDA(cudaMemsetAsync(s.status_dev, 0, sizeof(DevStatus), s.stream));
     TMD_CUDA(cudaMemsetAsync(s.thermo_dev, 0, 8 * sizeof(double), s.stream));
     ensure_scan_scratch(s, std::max(nseg, 26 * nblk));
+    return s.cnt && s.cstart && s.bmask && s.bcount && s.nbl && s.thermo_dev && s.status_dev;
 }
 
 bool require_alive(const char* what) {
@@ -590,7 +593,10 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.pend_final = s.pend_ghost = s.pend_kick = false;
     s.force_iters = s.rsq_iters = s.integration_iters = 0;
     s.launches = 0;
-    allocate_state(s, n, neighborlist_capacity);
+    if (!allocate_state(s, n, neighborlist_capacity)) {
+        free_all(s);
+        return -1;  // the error (a failed device allocation) is latched
+    }
 
     // core/grid.impala:215-249: the host mirror in input order
     s.h_mass.assign(masses, masses + n);

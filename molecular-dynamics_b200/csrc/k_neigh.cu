@@ -757,7 +757,7 @@ void run_enforce_pbc(State& s) {
     prof_end(K_PBC);
 }
 
-void grow_atoms(State& s, int need);  // api.cu
+bool grow_atoms(State& s, int need);  // api.cu
 
 void run_borders(State& s) {
     GeoArgs a = geo_args(s.geo);
@@ -793,7 +793,13 @@ void run_borders(State& s) {
     TMD_CUDA(cudaEventSynchronize(counted));
     const int G = s.status_host->nghost;
     if (N + G > s.capA) {
-        grow_atoms(s, N + G);
+        if (!grow_atoms(s, N + G)) {  // no room: no ghosts rather than writes past the arrays
+            s.G = 0;
+            s.lists_valid = 0;
+            s.tiles_valid = 0;
+            prof_end(K_BORDER);
+            return;
+        }
         emit();
     }
     prof_end(K_BORDER);
