@@ -131,6 +131,46 @@ def test_trajectory_exact_ghosts(product, oracle):
         oracle.oracle_set_ghost_mode(0)
 
 
+@pytest.mark.parametrize("mode", ["full", "exact_ghosts", "half"])
+def test_native_loop_matches_oracle(product, oracle, mode):
+    """md_run_timesteps, the loop the benchmark times (the force held back and joined with the next
+    initial integration and the ghost images; for half lists the final kick joined with it),
+    against the oracle's step-by-step calls over 60 steps (3 rebuilds): bit-identical with full
+    lists, to 1e-10 with half lists (reactions by atomics, another summation order).  The half
+    lists keep the periodic-boundary pairs: with the reference's half lists, which drop them, two
+    atoms can overlap across the boundary unrepelled until a wrap makes them list neighbours, and
+    the kick that follows throws one out of the grid (the oracle does the same)."""
+    if mode == "exact_ghosts":
+        product.md_set_ghost_mode(1)
+        oracle.oracle_set_ghost_mode(1)
+    half = mode == "half"
+    if half:
+        product.md_set_half_mode(1)
+        oracle.oracle_set_half_mode(1)
+    product.md_clear_error()
+    p, o = both(product, oracle, cells=(6, 6, 6), half=half)
+    try:
+        for chunk in range(3):
+            p.run(0.005, 20)
+            o.step(0.005, 20)
+            assert product.md_last_error() == 0, (chunk, product.md_last_error())
+            xp, vp, fp = tinymd.full_state(product)
+            xo, vo, fo = tinymd.full_state(oracle)
+            if half:
+                assert rel_err(xp, xo) < 1e-10 and rel_err(vp, vo) < 1e-10 and rel_err(fp, fo) < 1e-10
+            else:
+                np.testing.assert_array_equal(xp, xo, err_msg=f"positions after {20 * (chunk + 1)} steps")
+                np.testing.assert_array_equal(vp, vo)
+                np.testing.assert_array_equal(fp, fo)
+    finally:
+        close_all(p, o)
+        product.md_set_ghost_mode(0)
+        oracle.oracle_set_ghost_mode(0)
+        product.md_set_half_mode(0)
+        oracle.oracle_set_half_mode(0)
+        product.md_clear_error()
+
+
 def test_half_lists(product, oracle):
     p, o = both(product, oracle, cells=(8, 8, 8), half=True)
     try:
