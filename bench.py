@@ -70,12 +70,21 @@ def peaks():
 
 
 def measured_traffic():
-    """Per-launch DRAM bytes of the mixed force kernel from the committed ncu summary, if any."""
+    """Per-launch DRAM bytes of the mixed force kernel from the committed ncu summary, and its
+    L2 / L1 / issue fractions of peak from the same capture (None where absent)."""
     p = os.path.join(ROOT, "profiles", "force_lj_mixed_131k.json")
     if os.path.exists(p):
         with open(p) as f:
-            return json.load(f).get("dram_bytes_per_launch")
-    return None
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch"), {
+            "l2_sectors_per_launch": d.get("l2_sectors_per_launch"),
+            "l2_throughput_frac": (d["l2_throughput_pct_of_peak"] / 100.0 if "l2_throughput_pct_of_peak" in d
+                                   else None),
+            "l1_throughput_frac": (d["l1tex_throughput_pct_of_peak"] / 100.0
+                                   if "l1tex_throughput_pct_of_peak" in d else None),
+            "issue_frac": (d["sm_inst_executed_pct_of_peak"] / 100.0 if "sm_inst_executed_pct_of_peak" in d
+                           else None)}
+    return None, None
 
 
 class ClockSampler:
@@ -458,7 +467,7 @@ def run_ours(args):
     force_bytes, step_bytes = fused_kernel_bytes(mean_nb, ghosts_per_atom)
     bytes_per_atom = force_bytes + step_bytes
     achieved = natoms * bytes_per_atom / (force_ms * 1e-3) / 1e9
-    traffic = measured_traffic()
+    traffic, cache_fracs = measured_traffic()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms32 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -477,7 +486,9 @@ def run_ours(args):
                      # list count and entries plus the atom's own FP64 position and force: what
                      # must come from HBM once per step whatever the gathers hit
                      "compulsory_bytes_per_atom": 4 + 4 * mean_nb + 48,
-                     "compulsory_frac": natoms * (4 + 4 * mean_nb + 48) / (force_ms * 1e-3) / 1e9 / peak},
+                     "compulsory_frac": natoms * (4 + 4 * mean_nb + 48) / (force_ms * 1e-3) / 1e9 / peak,
+                     # from the ncu capture: the gathers hit L1/L2, and neither runs near its peak
+                     "ncu_fracs": cache_fracs},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
                 "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock",
