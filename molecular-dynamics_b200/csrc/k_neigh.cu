@@ -3,9 +3,9 @@
 //   * ghost generation (borders)     (comm/comm.impala:105-127, 528-642, 723-734; comm/lb.impala:88-100)
 //   * cell binning as a counting sort that reorders the device arrays by cell
 //                                    (core/grid.impala:280-321, 406-426)
-//   * neighbour-list build, one warp per cell, homes grouped by octant of the
-//     cell, candidates filtered by the octant's home bounding box, ballot/popc
-//     compaction                     (core/neighborlist.impala:1-78)
+//   * neighbour-list build, one warp per cell with a home atom per lane, the
+//     stencil's candidates filtered by the homes' bounding box and staged in
+//     shared memory               (core/neighborlist.impala:1-78)
 //
 // Ghost order.  The reference runs six passes (x+, x-, y+, y-, z+, z-); a
 // pass scans locals then all earlier ghosts in order and appends the ones
@@ -362,15 +362,27 @@ __device__ __forceinline__ int rel_cell(int k, int b) {
            ((wrap_diff(unpack_axis(k, 2), unpack_axis(b, 2)) + 128) << 16);
 }
 
+// Lane per home.  A warp takes one cell; its homes sit in lanes (32 at a time).  The 27
+// stencil cells' candidates (locals then ghosts per cell, stencil order) are staged in
+// shared memory, keeping only those within the list cutoff (with the FP32 margin) of the
+// bounding box of the homes, in order; then every lane walks the kept candidates (one
+// broadcast read each) and appends its own pairs, so each list comes out in stencil order
+// with no cross-lane compaction.  Lanes without a home sit far away and never match.
 #ifndef TMD_NL_WARPS
 #define TMD_NL_WARPS 4
 #endif
 #ifndef TMD_NL_TILE
-#define TMD_NL_TILE 256
+#define TMD_NL_TILE 128
 #endif
-constexpr int kNlWarps = TMD_NL_WARPS;  // warps (cells) per block
-constexpr int kTile = TMD_NL_TILE;      // staged candidates per warp and tile
-constexpr int kHomeMax = 64;            // home atoms handled per pass over the candidates
+#ifndef TMD_NL_MINB
+#define TMD_NL_MINB 8  // 64 registers: eight blocks of four warps per SM
+#endif
+#ifndef TMD_NL_UNROLL
+#define TMD_NL_UNROLL 4
+#endif
+constexpr int kNlWarps = TMD_NL_WARPS;    // warps (cells) per block
+constexpr int kNlTile = TMD_NL_TILE;      // kept candidates staged per warp before the homes walk them
+constexpr int kNlUnroll = TMD_NL_UNROLL;  // candidates per step of a home's walk
 
 struct NlArgs {
     double cut2;     // cutoff^2 (FP64, the reference's membership test)
@@ -380,21 +392,15 @@ struct NlArgs {
 };
 
 template <int HM>
-__global__ void __launch_bounds__(kNlWarps * 32)
+__global__ void __launch_bounds__(kNlWarps * 32, TMD_NL_MINB)
 k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
-             const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl,
-             DevStatus* st, NlArgs a) {
-    __shared__ float4 s_cpos[kNlWarps][kTile];  // candidate relative position, w = slot bits
-    __shared__ int s_cref[kNlWarps][HM ? kTile : 1];  // root reference indices (half modes only)
-    __shared__ int s_crbk[kNlWarps][kTile];
-    __shared__ float4 s_hpos[kNlWarps][kHomeMax];
-    __shared__ int s_hcnt[kNlWarps][kHomeMax];
+             const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl, DevStatus* st,
+             NlArgs a) {
+    __shared__ float4 s_cpos[kNlWarps][kNlTile];  // kept candidate position (cell-centre relative), w = slot
+    __shared__ int s_crel[kNlWarps][kNlTile];     // its rebasing cell relative to the first home's
+    __shared__ int s_cref[kNlWarps][HM ? kNlTile : 1];
     __shared__ int s_rstart[kNlWarps][54];
     __shared__ int s_rpre[kNlWarps][55];
-    __shared__ unsigned char s_oidx[kNlWarps][kTile];       // a tile's candidates kept for one octant
-    __shared__ float s_obox[kNlWarps][8][6];                // per octant: bounding box of its homes
-    __shared__ unsigned long long s_omask[kNlWarps][8];     // per octant: its homes (bits of the batch)
-    static_assert(kTile <= 256 && kHomeMax <= 64, "octant indices are bytes, home masks 64 bits");
 
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * kNlWarps + wid;
@@ -403,34 +409,34 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
     if (h0 == h1) return;
     const unsigned lt = lanemask_lt();
 
-    // 27 stencil cells in the reference order (z, y, x offsets -1..1), each
-    // contributing its locals then its ghosts: 54 ranges
-    int len = 0, start = 0;
-    if (lane < 27) {
-        int oz = lane / 9 - 1, oy = (lane / 3) % 3 - 1, ox = lane % 3 - 1;
-        int nb = c + oz * a.nxy + oy * a.nx + ox;
-        if (nb >= 0 && nb < a.ncells) {
-            start = cstart[nb];
-            len = cstart[nb + 1] - start;
-            int gs = cstart[a.ncells + 1 + nb];
+    // 27 stencil cells in the reference order (z, y, x offsets -1..1), each contributing
+    // its locals then its ghosts (54 ranges); lane l owns ranges 2l and 2l + 1
+    {
+        int start = 0, len = 0, gs = 0, gl = 0;
+        if (lane < 27) {
+            const int oz = lane / 9 - 1, oy = (lane / 3) % 3 - 1, ox = lane % 3 - 1;
+            const int nb = c + oz * a.nxy + oy * a.nx + ox;
+            if (nb >= 0 && nb < a.ncells) {
+                start = cstart[nb];
+                len = cstart[nb + 1] - start;
+                gs = cstart[a.ncells + 1 + nb];
+                gl = cstart[a.ncells + 2 + nb] - gs;
+            }
+        }
+        int incl = len + gl;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < 27) {
+            const int ex = incl - len - gl;
+            s_rstart[wid][2 * lane] = start;
             s_rstart[wid][2 * lane + 1] = gs;
-            s_rpre[wid][2 * lane + 1] = cstart[a.ncells + 2 + nb] - gs;  // ghost length (temporarily)
-        } else {
-            s_rstart[wid][2 * lane + 1] = 0;
-            s_rpre[wid][2 * lane + 1] = 0;
+            s_rpre[wid][2 * lane] = ex;
+            s_rpre[wid][2 * lane + 1] = ex + len;
         }
-        s_rstart[wid][2 * lane] = start;
-        s_rpre[wid][2 * lane] = len;
-    }
-    __syncwarp();
-    if (lane == 0) {
-        int acc = 0;
-        for (int q = 0; q < 54; ++q) {
-            int l = s_rpre[wid][q];
-            s_rpre[wid][q] = acc;
-            acc += l;
-        }
-        s_rpre[wid][54] = acc;
+        if (lane == 26) s_rpre[wid][54] = incl;
     }
     __syncwarp();
     const int M = s_rpre[wid][54];
@@ -438,166 +444,114 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
     const int cz = c / a.nxy, cy = (c / a.nx) % (a.nxy / a.nx), cx = c % a.nx;
     const double ctr[3] = {a.alo[0] + ((double)cx + 0.5) * a.spacing, a.alo[1] + ((double)cy + 0.5) * a.spacing,
                            a.alo[2] + ((double)cz + 0.5) * a.spacing};
-    int maxcnt = 0;
     const int rb0 = __ldg(rbk + h0);  // rebasing cells are staged relative to the first home's
+    int maxcnt = 0;
+    bool bad = false;
 
-    for (int hb = h0; hb < h1; hb += kHomeMax) {
-        const int hn = min(kHomeMax, h1 - hb);
-        for (int q = lane; q < hn; q += 32) {
-            double4 p = pos[hb + q];
-            s_hpos[wid][q] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]), (float)(p.z - ctr[2]), 0.0f);
-            s_hcnt[wid][q] = 0;
+    for (int hb = h0; hb < h1; hb += 32) {
+        const int hn = min(32, h1 - hb);
+        const bool home = lane < hn;
+        const int i = hb + (home ? lane : 0);
+        float hx = 1e18f, hy = 1e18f, hz = 1e18f;  // no home: never within the cutoff
+        int irel = 0, iref = 0;
+        if (home) {
+            const double4 p = pos[i];
+            hx = (float)(p.x - ctr[0]);
+            hy = (float)(p.y - ctr[1]);
+            hz = (float)(p.z - ctr[2]);
+            irel = rel_cell(rbk[i], rb0);
+            if (HM) iref = ref[i];
         }
-        __syncwarp();
-        {  // octant of each home (sign of its offset from the cell centre) and per-octant boxes
-            const bool v0 = lane < hn, v1 = lane + 32 < hn;
-            const float4 p0 = s_hpos[wid][v0 ? lane : 0], p1 = s_hpos[wid][v1 ? lane + 32 : 0];
-            const int o0 = (p0.x >= 0.f) | ((p0.y >= 0.f) << 1) | ((p0.z >= 0.f) << 2);
-            const int o1 = (p1.x >= 0.f) | ((p1.y >= 0.f) << 1) | ((p1.z >= 0.f) << 2);
-            for (int o = 0; o < 8; ++o) {
-                const bool in0 = v0 && o0 == o, in1 = v1 && o1 == o;
-                const unsigned m0 = __ballot_sync(0xffffffffu, in0), m1 = __ballot_sync(0xffffffffu, in1);
-                if ((m0 | m1) == 0u) {
-                    if (lane == 0) s_omask[wid][o] = 0ull;
-                    continue;
-                }
-                float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-                if (in0) {
-                    lo[0] = hi[0] = p0.x;
-                    lo[1] = hi[1] = p0.y;
-                    lo[2] = hi[2] = p0.z;
-                }
-                if (in1) {
-                    lo[0] = fminf(lo[0], p1.x), hi[0] = fmaxf(hi[0], p1.x);
-                    lo[1] = fminf(lo[1], p1.y), hi[1] = fmaxf(hi[1], p1.y);
-                    lo[2] = fminf(lo[2], p1.z), hi[2] = fmaxf(hi[2], p1.z);
-                }
+        // bounding box of the homes, widened by the list cutoff (with the FP32 margin)
+        float lo[3] = {home ? hx : INFINITY, home ? hy : INFINITY, home ? hz : INFINITY};
+        float hi[3] = {home ? hx : -INFINITY, home ? hy : -INFINITY, home ? hz : -INFINITY};
 #pragma unroll
-                for (int off = 16; off > 0; off >>= 1)
+        for (int off = 16; off > 0; off >>= 1)
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
-                        hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
-                    }
-                if (lane == 0) {
-                    s_omask[wid][o] = (unsigned long long)m0 | ((unsigned long long)m1 << 32);
-                    for (int d = 0; d < 3; ++d) {
-                        s_obox[wid][o][d] = lo[d];
-                        s_obox[wid][o][3 + d] = hi[d];
-                    }
-                }
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
+                hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
             }
-            __syncwarp();
-        }
-        for (int t0 = 0; t0 < M; t0 += kTile) {
-            const int tn = min(kTile, M - t0);
-            for (int m = t0 + lane; m < t0 + tn; m += 32) {
-                int lo = 0, hi = 53;  // the range of candidate m: the last one starting at or before m
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_rpre[wid][mid] <= m) lo = mid;
-                    else hi = mid - 1;
-                }
-                const int slot = s_rstart[wid][lo] + (m - s_rpre[wid][lo]);
-                double4 p = pos[slot];
-                s_cpos[wid][m - t0] = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]),
-                                                  (float)(p.z - ctr[2]), __int_as_float(slot));
-                if (HM) s_cref[wid][m - t0] = ref[slot];  // root reference index (ref for locals)
-                s_crbk[wid][m - t0] = rel_cell(rbk[slot], rb0);
-            }
-            __syncwarp();
-            // Homes are grouped by octant of their cell; a candidate is tested against an
-            // octant's homes only if it lies within the list cutoff (with the FP32 margin) of
-            // their bounding box.  Kept candidates stay in stencil order, so each home's list
-            // is the per-candidate test's, entry for entry.
-            for (int o = 0; o < 8; ++o) {
-                unsigned long long hm = s_omask[wid][o];
-                if (hm == 0ull) continue;
-                const float bx0 = s_obox[wid][o][0], by0 = s_obox[wid][o][1], bz0 = s_obox[wid][o][2];
-                const float bx1 = s_obox[wid][o][3], by1 = s_obox[wid][o][4], bz1 = s_obox[wid][o][5];
-                int nco = 0;
-                for (int q0 = 0; q0 < tn; q0 += 32) {
-                    const int q = q0 + lane;
-                    bool keep = false;
-                    if (q < tn) {
-                        const float4 cp = s_cpos[wid][q];
-                        const float ex = fmaxf(fmaxf(bx0 - cp.x, cp.x - bx1), 0.f);
-                        const float ey = fmaxf(fmaxf(by0 - cp.y, cp.y - by1), 0.f);
-                        const float ez = fmaxf(fmaxf(bz0 - cp.z, cp.z - bz1), 0.f);
-                        keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= a.hi2;
+        int cnt = 0;
+        int t0 = 0;  // next candidate to stage (M > 0: the home cell is in the stencil)
+        do {
+            int nk = 0;  // kept candidates staged (warp-uniform)
+            // stage: keep candidates in order until the next chunk might not fit
+            while (t0 < M && nk + 32 <= kNlTile) {
+                const int m = t0 + lane;
+                bool keep = false;
+                float4 cp;
+                int crel = 0, cref = 0;
+                if (m < M) {
+                    int lo_r = 0, hi_r = 53;  // the range of candidate m: the last one starting at or before m
+                    while (lo_r < hi_r) {
+                        const int mid = (lo_r + hi_r + 1) >> 1;
+                        if (s_rpre[wid][mid] <= m) lo_r = mid;
+                        else hi_r = mid - 1;
                     }
-                    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                    const int slot = s_rstart[wid][lo_r] + (m - s_rpre[wid][lo_r]);
+                    const double4 p = pos[slot];
+                    cp = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]), (float)(p.z - ctr[2]),
+                                     __int_as_float(slot));
+                    const float ex = fmaxf(fmaxf(lo[0] - cp.x, cp.x - hi[0]), 0.f);
+                    const float ey = fmaxf(fmaxf(lo[1] - cp.y, cp.y - hi[1]), 0.f);
+                    const float ez = fmaxf(fmaxf(lo[2] - cp.z, cp.z - hi[2]), 0.f);
+                    keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= a.hi2;
                     if (keep) {
-                        const int at = nco + __popc(bal & lt);
-                        s_oidx[wid][at] = (unsigned char)q;
+                        crel = rel_cell(rbk[slot], rb0);
+                        if (HM) cref = ref[slot];  // root reference index (ref for locals)
                     }
-                    nco += __popc(bal);
                 }
-                __syncwarp();
-                while (hm) {
-                    const int h = __ffsll((long long)hm) - 1;
-                    hm &= hm - 1ull;
-                    const int i = hb + h;
-                    const float4 hp = s_hpos[wid][h];
-                    const int iref = HM ? ref[i] : 0;
-                    const int irel = rel_cell(rbk[i], rb0);
-                    int cnt = s_hcnt[wid][h];
-                    for (int q0 = 0; q0 < nco; q0 += 32) {
-                        const int qq = q0 + lane;
-                        bool pred = false;
-                        int slot = -1;
-                        int code = 0;
-                        if (qq < nco) {
-                            const int q = s_oidx[wid][qq];
-                            const float4 cp = s_cpos[wid][q];
-                            slot = __float_as_int(cp.w);
-                            const float dx = hp.x - cp.x, dy = hp.y - cp.y, dz = hp.z - cp.z;
-                            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                            bool in = r2 < a.lo2;
-                            if (!in && r2 <= a.hi2) {
-                                // near the cutoff: the reference's exact FP64 test
-                                const double4 pi = pos[i], pj = pos[slot];
-                                in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
-                            }
-                            // core/neighborlist.impala:34: half lists keep i > j (reference index);
-                            // HM == 2 compares ghosts by their root so pairs across the periodic
-                            // boundary are kept once
-                            pred = in && slot != i && (!HM || s_cref[wid][HM ? q : 0] < iref);
-                            if (pred) {
-                                // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow
-                                // shows up as bits above bit 1 or in byte 3) means |dk| > 1
-                                const uint32_t d = (uint32_t)(s_crbk[wid][q] - irel + 0x010101);
-                                if ((d & 0xFFFCFCFCu) || (d & (d >> 1) & 0x010101u)) {
-                                    atomicAdd(&st->bad_code, 1);
-                                    code = 21;  // dk = 0
-                                } else {
-                                    code = (int)((d & 3u) | ((d >> 6) & 0xCu) | ((d >> 12) & 0x30u));
-                                }
-                            }
-                        }
-                        const unsigned bal = __ballot_sync(0xffffffffu, pred);
-                        if (pred) {
-                            const int p = cnt + __popc(bal & lt);
-                            if (p < a.nbcap) nbl[(size_t)p * a.stride + i] = ((uint32_t)slot << kCodeBits) | (uint32_t)code;
-                        }
-                        cnt += __popc(bal);
-                    }
-                    if (lane == 0) s_hcnt[wid][h] = cnt;
-                    __syncwarp();
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int at = nk + __popc(bal & lt);
+                    s_cpos[wid][at] = cp;
+                    s_crel[wid][at] = crel;
+                    if (HM) s_cref[wid][at] = cref;
                 }
-                __syncwarp();
+                nk += __popc(bal);
+                t0 += 32;
             }
             __syncwarp();
+            // every home walks the kept candidates in order
+#pragma unroll kNlUnroll
+            for (int k = 0; k < nk; ++k) {
+                const float4 cp = s_cpos[wid][k];
+                const float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const int slot = __float_as_int(cp.w);
+                bool in = r2 < a.lo2;
+                if (!in && r2 <= a.hi2) {
+                    // near the cutoff: the reference's exact FP64 test
+                    const double4 pi = pos[i], pj = pos[slot];
+                    in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
+                }
+                // core/neighborlist.impala:34: half lists keep i > j (reference index); HM == 2
+                // compares ghosts by their root so pairs across the periodic boundary are kept once
+                if (in && slot != i && (!HM || s_cref[wid][HM ? k : 0] < iref)) {
+                    // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow shows up as
+                    // bits above bit 1 or in byte 3) means |dk| > 1
+                    const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
+                    const bool b = (d & 0xFFFCFCFCu) || (d & (d >> 1) & 0x010101u);
+                    bad |= b;
+                    const uint32_t code = b ? 21u : ((d & 3u) | ((d >> 6) & 0xCu) | ((d >> 12) & 0x30u));
+                    if (cnt < a.nbcap) nbl[(size_t)cnt * a.stride + i] = ((uint32_t)slot << kCodeBits) | code;
+                    ++cnt;
+                }
+            }
+            __syncwarp();
+        } while (t0 < M);
+        if (home) {
+            nbn[i] = cnt;
+            maxcnt = max(maxcnt, cnt);
         }
-        for (int q = lane; q < hn; q += 32) {
-            const int n = s_hcnt[wid][q];
-            nbn[hb + q] = n;
-            maxcnt = max(maxcnt, n);
-        }
-        __syncwarp();
     }
     maxcnt = warp_max(maxcnt);
-    if (lane == 0) atomicMax(&st->max_nb, maxcnt);
+    const unsigned nbad = __popc(__ballot_sync(0xffffffffu, bad));
+    if (lane == 0) {
+        atomicMax(&st->max_nb, maxcnt);
+        if (nbad) atomicAdd(&st->bad_code, (int)nbad);
+    }
 }
 
 // Locals outside the grid (bucket ncells) get empty lists.
@@ -885,13 +839,13 @@ int run_build_lists(State& s, bool half, double cutoff) {
         if (!use_tiles) {
             if (half && s.half_ghost)
                 k_build_list<2><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart,
-                                                                    s.nbn, s.nbl, s.status_dev, a);
+                                                                        s.nbn, s.nbl, s.status_dev, a);
             else if (half)
-                k_build_list<1><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                    s.nbn, s.nbl, s.status_dev, a);
+                k_build_list<1><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk,
+                                                                        s.cstart, s.nbn, s.nbl, s.status_dev, a);
             else
-                k_build_list<0><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                    s.nbn, s.nbl, s.status_dev, a);
+                k_build_list<0><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk,
+                                                                        s.cstart, s.nbn, s.nbl, s.status_dev, a);
         }
         launched(K_NLIST);
         prof_end(K_NLIST);

@@ -451,7 +451,9 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
         int ncnt = 0;
         int nq = 0, q0 = 0, q1 = 0;  // deferred FP64 pairs
         const uint32_t* lp = nbl + i;
-        const uint32_t pad = ((uint32_t)i << kCodeBits) | 21u;  // the atom itself, masked below
+        // padding: the atom itself one rebasing cell away on every axis (rsq = 3h^2 with h above
+        // the list cutoff, beyond every window), so it is neither a fast nor a queued pair
+        const uint32_t pad = ((uint32_t)i << kCodeBits) | 42u;
         uint32_t ent[kB32];
 #pragma unroll
         for (int u = 0; u < kB32; ++u) ent[u] = u < n ? __ldg(lp + (size_t)u * a.stride) : pad;
@@ -479,8 +481,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
                 const float dz = fmaf(a.hz, sz, ri.z - rj[u].z);
                 const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const bool fast = rsq < a.rc2_lo && rsq >= a.close2;
-                // padding (the atom itself: rsq = 0) is neither fast nor queued
-                slow |= (!fast && rsq < a.rc2_hi && k0 + u < n) ? (1u << u) : 0u;
+                slow |= (!fast && rsq < a.rc2_hi) ? (1u << u) : 0u;
                 float sr2;
                 asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
                 const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
@@ -966,6 +967,15 @@ void run_reduce_partials(State& s, int nb, int q0, int q1) {
     launched(K_REDUCE);
 }
 
+// The mixed kernel pads a batch with the atom itself one rebasing cell away on every
+// axis (rsq = 3h^2), which must lie beyond the cutoff window; h exceeds the cell
+// spacing, so only a cutoff beyond sqrt(3) cell spacings (where the 27-cell stencil
+// misses pairs anyway) breaks this.  Latches MD_ERR_ARGUMENT (3).
+void check_mixed_cutoff(const State& s, const LjArgs& a) {
+    if (3.0 * s.geo.rb_h * s.geo.rb_h <= (double)a.rc2_hi)
+        set_error(3, "mixed form: LJ cutoff beyond sqrt(3) cell spacings");
+}
+
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
     const int N = s.N;
     if (N == 0) return;
@@ -974,6 +984,7 @@ void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
         return;
     }
     LjArgs a = lj_args(s, p, dt);
+    if (s.precision == 1 && !p.half) check_mixed_cutoff(s, a);
     // the list entry's code holds dk + 1 in bits 0-1 (x), 2-3 (y), 4-5 (z)
     a.hx = (float)(-s.geo.rb_h);
     a.hy = (float)(-s.geo.rb_h / 4.0);
@@ -1024,6 +1035,7 @@ void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double 
     const int N = s.N;
     if (N == 0) return;  // no ghosts either
     LjArgs a = lj_args(s, p, dt_final);
+    if (s.precision == 1) check_mixed_cutoff(s, a);
     a.hx = (float)(-s.geo.rb_h);
     a.hy = (float)(-s.geo.rb_h / 4.0);
     a.hz = (float)(-s.geo.rb_h / 16.0);
