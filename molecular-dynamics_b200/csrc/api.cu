@@ -234,6 +234,7 @@ std::vector<SlabItem> slab_items(State& s) {
     for (int** q : scratch) v.push_back(item(q, 1, false));
     v.push_back(item(&s.img_cnt, 2, false));
     v.push_back(item(&s.img_slot, kImgW, false));
+    v.push_back(item(&s.dl_buf, 10, false));  // host-mirror transfers: mass, pos[3], vel[3], frc[3]
     return v;
 }
 
@@ -242,8 +243,6 @@ void free_all(State& s) {
     dfree(&s.slab);
     int** ip[] = {&s.cnt, &s.cstart, &s.bcount, &s.scan_part, &s.tile_desc, &s.tile_rows};
     for (int** q : ip) dfree(q);
-    dfree(&s.dl_buf);
-    s.dl_cap = 0;
     s.img_ok = 0;
     s.ghosts_pushed = 0;
     dfree(&s.bmask);
@@ -403,19 +402,6 @@ void flush_all(State& s) {
 
 void sync_stream(State& s) { TMD_CUDA(cudaStreamSynchronize(s.stream)); }
 
-// pinned staging area for host <-> device copies
-void* stage_ptr = nullptr;
-size_t stage_bytes = 0;
-void* stage(size_t bytes) {
-    if (bytes > stage_bytes) {
-        if (stage_ptr) cudaFreeHost(stage_ptr);
-        stage_ptr = nullptr;
-        stage_bytes = bytes + (bytes >> 3) + 4096;
-        if (!TMD_CUDA(cudaMallocHost(&stage_ptr, stage_bytes))) stage_bytes = 0;
-    }
-    return stage_ptr;
-}
-
 // device state -> the host mirror's layout, by reference index r (a permutation of the slots):
 // out = mass[NA], pos[NA][3], vel[NA][3], frc[NA][3]; ghost velocities only for the
 // contact-fixed DEM model, ghost forces zero (what md_copy_data_from_accelerator reports)
@@ -456,13 +442,23 @@ __global__ void k_gather_ref(const double4* __restrict__ pos, const double4* __r
     of[3 * (size_t)r + 2] = fz;
 }
 
-__global__ void k_iota(int* a, int* b, int* img, int n) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        a[i] = i;
-        b[i] = i;
-        img[i] = 0;
-    }
+// host mirror (input order: mass[n], pos[n][3], vel[n][3]) -> slot arrays, slot = reference
+// index; forces zero, no wraps yet
+__global__ void k_upload(const double* __restrict__ m, const double* __restrict__ p, const double* __restrict__ v,
+                         double4* __restrict__ pos, double4* __restrict__ vel, double4* __restrict__ frc,
+                         float4* __restrict__ frc32, double* __restrict__ mass, int* __restrict__ ref,
+                         int* __restrict__ slot_of_ref, int* __restrict__ img, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const size_t k = 3 * (size_t)i;
+    pos[i] = make_double4(p[k], p[k + 1], p[k + 2], 0.0);
+    vel[i] = make_double4(v[k], v[k + 1], v[k + 2], 0.0);
+    frc[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+    frc32[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    mass[i] = m[i];
+    ref[i] = i;
+    slot_of_ref[i] = i;
+    img[i] = 0;
 }
 
 __global__ void k_convert_forces(double4* f64, float4* f32, int n, int to32) {
@@ -599,19 +595,19 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     }
 
     // core/grid.impala:215-249: the host mirror in input order
-    s.h_mass.assign(masses, masses + n);
+    static_assert(sizeof(Vector3D) == 3 * sizeof(double), "Vector3D is three packed doubles");
+    s.h_mass.resize(n);
     s.h_pos.resize((size_t)n * 3);
     s.h_vel.resize((size_t)n * 3);
-    s.h_frc.assign((size_t)n * 3, 0.0);
-    for (int i = 0; i < n; ++i) {
-        s.h_pos[3 * i + 0] = positions[i].x;
-        s.h_pos[3 * i + 1] = positions[i].y;
-        s.h_pos[3 * i + 2] = positions[i].z;
-        s.h_vel[3 * i + 0] = velocities[i].x;
-        s.h_vel[3 * i + 1] = velocities[i].y;
-        s.h_vel[3 * i + 2] = velocities[i].z;
+    s.h_frc.resize((size_t)n * 3);
+    s.h_x0.resize((size_t)n * 3);
+    if (n > 0) {
+        std::memcpy(s.h_mass.data(), masses, sizeof(double) * n);
+        std::memcpy(s.h_pos.data(), positions, sizeof(Vector3D) * n);
+        std::memcpy(s.h_vel.data(), velocities, sizeof(Vector3D) * n);
+        std::memset(s.h_frc.data(), 0, sizeof(Vector3D) * n);
+        std::memcpy(s.h_x0.data(), positions, sizeof(Vector3D) * n);
     }
-    s.h_x0 = s.h_pos;
     s.alive = true;
     phase_reset();
     return s.N;
@@ -643,24 +639,18 @@ void md_copy_data_to_accelerator(void) {
     s.G = 0;
     s.pc = s.vc = s.ac = 0;
     if (N == 0) return;
-    double4* st = (double4*)stage(sizeof(double4) * (size_t)N * 2 + sizeof(double) * N);
-    if (!st) return;
-    double4* sp = st;
-    double4* sv = st + N;
-    double* sm = (double*)(st + 2 * (size_t)N);
-    for (int i = 0; i < N; ++i) {
-        sp[i] = make_double4(s.h_pos[3 * i], s.h_pos[3 * i + 1], s.h_pos[3 * i + 2], 0.0);
-        sv[i] = make_double4(s.h_vel[3 * i], s.h_vel[3 * i + 1], s.h_vel[3 * i + 2], 0.0);
-        sm[i] = s.h_mass[i];
-    }
-    TMD_CUDA(cudaMemcpyAsync(s.pos.b[0], sp, sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
-    TMD_CUDA(cudaMemcpyAsync(s.vel.b[0], sv, sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
-    TMD_CUDA(cudaMemcpyAsync(s.mass.b[0], sm, sizeof(double) * N, cudaMemcpyHostToDevice, s.stream));
-    TMD_CUDA(cudaMemsetAsync(s.frc.b[0], 0, sizeof(double4) * N, s.stream));
-    TMD_CUDA(cudaMemsetAsync(s.frc32, 0, sizeof(float4) * N, s.stream));
-    k_iota<<<(N + 255) / 256, 256, 0, s.stream>>>(s.ref.b[0], s.slot_of_ref, s.img.b[0], N);
+    // the mirror (page-locked, reference order = input order here) goes up as it is and is
+    // spread into the slot arrays on the device
+    double* dm = s.dl_buf;
+    double* dp = s.dl_buf + N;
+    double* dv = s.dl_buf + 4 * (size_t)N;
+    TMD_CUDA(cudaMemcpyAsync(dm, s.h_mass.data(), sizeof(double) * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(dp, s.h_pos.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(dv, s.h_vel.data(), sizeof(double) * 3 * N, cudaMemcpyHostToDevice, s.stream));
+    k_upload<<<(N + 255) / 256, 256, 0, s.stream>>>(dm, dp, dv, s.pos.b[0], s.vel.b[0], s.frc.b[0], s.frc32,
+                                                    s.mass.b[0], s.ref.b[0], s.slot_of_ref, s.img.b[0], N);
     launched(K_MISC);
-    // the staging area is reused by later calls: wait for the copies
+    // the mirror may be resized (and moved) by later calls: wait for the copies out of it
     sync_stream(s);
 }
 
@@ -676,25 +666,20 @@ void md_copy_data_from_accelerator(void) {
     s.h_vel.resize((size_t)NA * 3);
     s.h_frc.resize((size_t)NA * 3);
     if (NA == 0) return;
-    // gathered into reference order on the device, one copy into pinned memory
-    const size_t words = (size_t)10 * NA;
-    if (words > s.dl_cap) {
-        dfree(&s.dl_buf);
-        s.dl_cap = words + words / 8 + 1024;
-        dalloc(&s.dl_buf, s.dl_cap);
-    }
-    double* host = (double*)stage(sizeof(double) * words);
-    if (!host) return;
+    // gathered into reference order on the device, copied straight into the page-locked mirror
     k_gather_ref<<<(NA + 255) / 256, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.frc32,
                                                          s.mass.b[s.ac], s.ref.b[s.ac], s.dl_buf, s.N, NA,
                                                          s.precision == 1, s.dem_fixed);
     launched(K_MISC);
-    TMD_CUDA(cudaMemcpyAsync(host, s.dl_buf, sizeof(double) * words, cudaMemcpyDeviceToHost, s.stream));
+    const size_t na = (size_t)NA;
+    TMD_CUDA(cudaMemcpyAsync(s.h_mass.data(), s.dl_buf, sizeof(double) * na, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(s.h_pos.data(), s.dl_buf + na, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost,
+                             s.stream));
+    TMD_CUDA(cudaMemcpyAsync(s.h_vel.data(), s.dl_buf + 4 * na, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost,
+                             s.stream));
+    TMD_CUDA(cudaMemcpyAsync(s.h_frc.data(), s.dl_buf + 7 * na, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost,
+                             s.stream));
     sync_stream(s);
-    std::copy(host, host + NA, s.h_mass.begin());
-    std::copy(host + NA, host + 4 * (size_t)NA, s.h_pos.begin());
-    std::copy(host + 4 * (size_t)NA, host + 7 * (size_t)NA, s.h_vel.begin());
-    std::copy(host + 7 * (size_t)NA, host + 10 * (size_t)NA, s.h_frc.begin());
 }
 
 void md_exchange_particles(void) {  // comm/comm.impala:392-525: no remote ranks in one process
@@ -856,11 +841,12 @@ int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* 
     State& s = g_state;
     if (!require_alive("md_write_grid_data_to_arrays")) return 0;
     flush_all(s);
-    for (int i = 0; i < s.N && (size_t)3 * i + 2 < s.h_pos.size(); ++i) {
-        m[i] = s.h_mass[i];
-        x[i] = Vector3D{s.h_pos[3 * i], s.h_pos[3 * i + 1], s.h_pos[3 * i + 2]};
-        v[i] = Vector3D{s.h_vel[3 * i], s.h_vel[3 * i + 1], s.h_vel[3 * i + 2]};
-        f[i] = Vector3D{s.h_frc[3 * i], s.h_frc[3 * i + 1], s.h_frc[3 * i + 2]};
+    const size_t n = std::min((size_t)s.N, s.h_mass.size());
+    if (n > 0) {
+        std::memcpy(m, s.h_mass.data(), sizeof(double) * n);
+        std::memcpy(x, s.h_pos.data(), sizeof(Vector3D) * n);
+        std::memcpy(v, s.h_vel.data(), sizeof(Vector3D) * n);
+        std::memcpy(f, s.h_frc.data(), sizeof(Vector3D) * n);
     }
     return s.N;
 }
@@ -871,12 +857,13 @@ int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vect
     if (!require_alive("md_write_grid_ghost_data_to_arrays")) return 0;
     flush_all(s);
     const size_t have = s.h_mass.size();
-    for (int g = 0; g < s.G && (size_t)(s.N + g) < have; ++g) {
-        const size_t p = (size_t)s.N + g;
-        m[g] = s.h_mass[p];
-        x[g] = Vector3D{s.h_pos[3 * p], s.h_pos[3 * p + 1], s.h_pos[3 * p + 2]};
-        v[g] = Vector3D{s.h_vel[3 * p], s.h_vel[3 * p + 1], s.h_vel[3 * p + 2]};
-        f[g] = Vector3D{s.h_frc[3 * p], s.h_frc[3 * p + 1], s.h_frc[3 * p + 2]};
+    const size_t n0 = (size_t)s.N;
+    const size_t ng = have > n0 ? std::min((size_t)s.G, have - n0) : 0;
+    if (ng > 0) {
+        std::memcpy(m, s.h_mass.data() + n0, sizeof(double) * ng);
+        std::memcpy(x, s.h_pos.data() + 3 * n0, sizeof(Vector3D) * ng);
+        std::memcpy(v, s.h_vel.data() + 3 * n0, sizeof(Vector3D) * ng);
+        std::memcpy(f, s.h_frc.data() + 3 * n0, sizeof(Vector3D) * ng);
     }
     return s.N;
 }

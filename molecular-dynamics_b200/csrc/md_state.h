@@ -6,10 +6,53 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
+#include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace tmd {
+
+// Page-locked host memory for the host mirror, so host<->device copies go straight
+// to and from it.  New elements are left uninitialised (every user overwrites them),
+// and a failed page-locked allocation falls back to ordinary memory (the copies
+// then stage through the driver); a 64-byte header records which kind a block is.
+template <class T>
+struct PinnedAlloc {
+    using value_type = T;
+    PinnedAlloc() = default;
+    template <class U>
+    PinnedAlloc(const PinnedAlloc<U>&) {}
+    T* allocate(size_t n) {
+        const size_t bytes = n * sizeof(T) + kHeader;
+        void* p = nullptr;
+        int kind = 1;
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            p = std::malloc(bytes);
+            kind = 2;
+            if (!p) throw std::bad_alloc();
+        }
+        *(int*)p = kind;
+        return (T*)((char*)p + kHeader);
+    }
+    void deallocate(T* q, size_t) {
+        void* p = (char*)q - kHeader;
+        if (*(int*)p == 2) std::free(p);
+        else if (cudaFreeHost(p) != cudaSuccess) cudaGetLastError();  // runtime already unloading: leave it
+    }
+    template <class U>
+    void construct(U* p) noexcept { ::new ((void*)p) U; }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) { ::new ((void*)p) U(std::forward<A>(a)...); }
+    static constexpr size_t kHeader = 64;
+};
+template <class T, class U>
+bool operator==(const PinnedAlloc<T>&, const PinnedAlloc<U>&) { return true; }
+template <class T, class U>
+bool operator!=(const PinnedAlloc<T>&, const PinnedAlloc<U>&) { return false; }
+using HostVec = std::vector<double, PinnedAlloc<double>>;
 
 enum Phase { PH_FORCE = 1, PH_NEIGH = 2, PH_COMM = 3, PH_BALANCE = 4, PH_OTHER = 5, PH_COUNT = 6 };
 
@@ -128,8 +171,7 @@ struct State {
     // ghost images by local (k_ghost_links at every distribution): the force kernel that does
     // the next initial integration writes them, so no separate ghost refresh is needed
     char* slab = nullptr;      // the one allocation the per-slot arrays are carved from (grow_atoms)
-    double* dl_buf = nullptr;  // md_copy_data_from_accelerator's gather (mass, pos, vel, frc by reference)
-    size_t dl_cap = 0;         // its capacity in doubles
+    double* dl_buf = nullptr;  // host-mirror transfers (mass, pos, vel, frc by reference): 10 doubles per slot
     int* img_cnt = nullptr;    // [2][capA]: direct two-phase images of a local, all its images
     int* img_slot = nullptr;   // [kImgW][capA]: their slots by plane (kImg1 two-phase planes, then
                                // kImg2 exact ones), -1 after a local's last image
@@ -167,9 +209,9 @@ struct State {
     double* thermo_host = nullptr;     // pinned [8]
 
     // host mirror in reference order (core/grid.impala ArrayData host buffers)
-    std::vector<double> h_mass;                 // [N+G]
-    std::vector<double> h_pos, h_vel, h_frc;    // [(N+G)*3]
-    std::vector<double> h_x0;                   // initial positions (adjoint)
+    HostVec h_mass;                 // [N+G]
+    HostVec h_pos, h_vel, h_frc;    // [(N+G)*3]
+    HostVec h_x0;                   // initial positions (adjoint)
 
     PendingForce pend_force;
     PendingForce force_cfg;   // parameters of the last md_compute_* call

@@ -288,7 +288,8 @@ class Simulation:
         """(masses, positions, velocities, forces) of the locals via md_copy_data_from_accelerator."""
         self.lib.md_copy_data_from_accelerator()
         n = self.n
-        m, x, v, f = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+        # every element is written by md_write_grid_data_to_arrays
+        m, x, v, f = np.empty(n), np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
         self.lib.md_write_grid_data_to_arrays(ptr(m), ptr(x), ptr(v), ptr(f))
         check(self.lib)
         return m, x, v, f
