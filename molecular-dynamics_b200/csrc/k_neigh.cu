@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(kNlWarps * 32, TMD_NL_MINB)
 k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
              const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl, DevStatus* st,
              NlArgs a) {
-    __shared__ float4 s_cpos[kNlWarps][kNlTile];  // kept candidate position (cell-centre relative), w = slot
+    __shared__ float4 s_cpos[kNlWarps][kNlTile];  // kept candidate position (cell-centre relative), w = slot << 6
     __shared__ int s_crel[kNlWarps][kNlTile];     // its rebasing cell relative to the first home's
     __shared__ int s_cref[kNlWarps][HM ? kNlTile : 1];
     __shared__ int s_rstart[kNlWarps][54];
@@ -446,12 +446,15 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                            a.alo[2] + ((double)cz + 0.5) * a.spacing};
     const int rb0 = __ldg(rbk + h0);  // rebasing cells are staged relative to the first home's
     int maxcnt = 0;
-    bool bad = false;
+    // per-axis bytes dk + 1 of the pairs written, OR-ed: a byte outside 0..2 (a borrow shows up
+    // as bits above bit 1 or in byte 3; a 3 becomes 4 when 1 is added) means |dk| > 1
+    uint32_t dk_or = 0, dk1_or = 0;
 
     for (int hb = h0; hb < h1; hb += 32) {
         const int hn = min(32, h1 - hb);
         const bool home = lane < hn;
         const int i = hb + (home ? lane : 0);
+        const uint32_t i6 = (uint32_t)i << kCodeBits;
         float hx = 1e18f, hy = 1e18f, hz = 1e18f;  // no home: never within the cutoff
         int irel = 0, iref = 0;
         if (home) {
@@ -492,7 +495,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                     const int slot = s_rstart[wid][lo_r] + (m - s_rpre[wid][lo_r]);
                     const double4 p = pos[slot];
                     cp = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]), (float)(p.z - ctr[2]),
-                                     __int_as_float(slot));
+                                     __uint_as_float((uint32_t)slot << kCodeBits));
                     const float ex = fmaxf(fmaxf(lo[0] - cp.x, cp.x - hi[0]), 0.f);
                     const float ey = fmaxf(fmaxf(lo[1] - cp.y, cp.y - hi[1]), 0.f);
                     const float ez = fmaxf(fmaxf(lo[2] - cp.z, cp.z - hi[2]), 0.f);
@@ -519,23 +522,23 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 const float4 cp = s_cpos[wid][k];
                 const float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const int slot = __float_as_int(cp.w);
+                const uint32_t s6 = __float_as_uint(cp.w);  // slot << 6
                 bool in = r2 < a.lo2;
                 if (!in && r2 <= a.hi2) {
                     // near the cutoff: the reference's exact FP64 test
-                    const double4 pi = pos[i], pj = pos[slot];
+                    const double4 pi = pos[i], pj = pos[s6 >> kCodeBits];
                     in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
                 }
                 // core/neighborlist.impala:34: half lists keep i > j (reference index); HM == 2
                 // compares ghosts by their root so pairs across the periodic boundary are kept once
-                if (in && slot != i && (!HM || s_cref[wid][HM ? k : 0] < iref)) {
-                    // dk + 1 per axis in bytes 0-2; any byte outside 0..2 (a borrow shows up as
-                    // bits above bit 1 or in byte 3) means |dk| > 1
+                if (in && s6 != i6 && (!HM || s_cref[wid][HM ? k : 0] < iref)) {
+                    // dk + 1 per axis in bytes 0-2, packed as x | y << 2 | z << 4 (the three
+                    // shifted copies land in disjoint bits 0-5 without carries)
                     const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
-                    const bool b = (d & 0xFFFCFCFCu) || (d & (d >> 1) & 0x010101u);
-                    bad |= b;
-                    const uint32_t code = b ? 21u : ((d & 3u) | ((d >> 6) & 0xCu) | ((d >> 12) & 0x30u));
-                    if (cnt < a.nbcap) nbl[(size_t)cnt * a.stride + i] = ((uint32_t)slot << kCodeBits) | code;
+                    dk_or |= d;
+                    dk1_or |= d + 0x010101u;
+                    const uint32_t code = (d + (d >> 6) + (d >> 12)) & 63u;
+                    if (cnt < a.nbcap) nbl[(size_t)cnt * a.stride + i] = s6 | code;
                     ++cnt;
                 }
             }
@@ -547,6 +550,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
         }
     }
     maxcnt = warp_max(maxcnt);
+    const bool bad = ((dk_or & 0xFFFCFCFCu) | (dk1_or & 0x040404u)) != 0u;
     const unsigned nbad = __popc(__ballot_sync(0xffffffffu, bad));
     if (lane == 0) {
         atomicMax(&st->max_nb, maxcnt);
