@@ -531,7 +531,18 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 }
                 // core/neighborlist.impala:34: half lists keep i > j (reference index); HM == 2
                 // compares ghosts by their root so pairs across the periodic boundary are kept once
-                if (in && s6 != i6 && (!HM || s_cref[wid][HM ? k : 0] < iref)) {
+                const bool take = in && s6 != i6 && (!HM || s_cref[wid][HM ? k : 0] < iref);
+                if (HM) {
+                    // half lists: the append without a branch (measured faster there, while
+                    // the full-list walk is faster with the branch)
+                    const uint32_t d0 = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
+                    const uint32_t d = take ? d0 : 0x010101u;
+                    dk_or |= d;
+                    dk1_or |= d + 0x010101u;
+                    const uint32_t code = (d + (d >> 6) + (d >> 12)) & 63u;
+                    if (take && cnt < a.nbcap) nbl[(size_t)cnt * a.stride + i] = s6 | code;
+                    cnt += take ? 1 : 0;
+                } else if (take) {
                     // dk + 1 per axis in bytes 0-2, packed as x | y << 2 | z << 4 (the three
                     // shifted copies land in disjoint bits 0-5 without carries)
                     const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
