@@ -400,6 +400,15 @@ void flush_all(State& s) {
     flush_force(s);
 }
 
+// everything but the carried-over ghosts: for calls that touch only the locals, so that a
+// following md_borders, which writes every ghost anew, can drop the carry
+void flush_locals(State& s) {
+    flush_final(s);
+    flush_init(s);
+    flush_kick(s);
+    flush_force(s);
+}
+
 void sync_stream(State& s) { TMD_CUDA(cudaStreamSynchronize(s.stream)); }
 
 // device state -> the host mirror's layout, by reference index r (a permutation of the slots):
@@ -683,13 +692,13 @@ void md_copy_data_from_accelerator(void) {
 }
 
 void md_exchange_particles(void) {  // comm/comm.impala:392-525: no remote ranks in one process
-    if (require_alive("md_exchange_particles")) flush_all(g_state);
+    if (require_alive("md_exchange_particles")) flush_locals(g_state);
 }
 
-void md_enforce_pbc(void) {
+void md_enforce_pbc(void) {  // wraps locals only: a pending ghost carry stays pending
     State& s = g_state;
     if (!require_alive("md_enforce_pbc")) return;
-    flush_all(s);
+    flush_locals(s);
     phase_mark(PH_OTHER);
     run_enforce_pbc(s);
 }
@@ -697,6 +706,7 @@ void md_enforce_pbc(void) {
 void md_borders(void) {
     State& s = g_state;
     if (!require_alive("md_borders")) return;
+    s.pend_ghost = false;  // every ghost is written anew below: the carry would be overwritten
     flush_all(s);
     phase_mark(PH_COMM);
     run_borders(s);
