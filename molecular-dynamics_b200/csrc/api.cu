@@ -392,12 +392,20 @@ void flush_ghost(State& s) {
     run_ghost_refresh(s, 0);
 }
 
+void flush_pbc(State& s) {
+    if (!s.pend_pbc) return;
+    s.pend_pbc = false;
+    phase_mark(PH_OTHER);
+    run_enforce_pbc(s);
+}
+
 void flush_all(State& s) {
     flush_final(s);
     flush_ghost(s);
     flush_init(s);
     flush_kick(s);
     flush_force(s);
+    flush_pbc(s);
 }
 
 // everything but the carried-over ghosts: for calls that touch only the locals, so that a
@@ -407,6 +415,7 @@ void flush_locals(State& s) {
     flush_init(s);
     flush_kick(s);
     flush_force(s);
+    flush_pbc(s);
 }
 
 void sync_stream(State& s) { TMD_CUDA(cudaStreamSynchronize(s.stream)); }
@@ -595,7 +604,8 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.lists_valid = 0;
     s.pend_init = false;
     s.pend_force = PendingForce();
-    s.pend_final = s.pend_ghost = s.pend_kick = false;
+    s.pend_final = s.pend_ghost = s.pend_kick = s.pend_pbc = false;
+    s.bin_zeroed = s.build_zeroed = false;
     s.force_iters = s.rsq_iters = s.integration_iters = 0;
     s.launches = 0;
     if (!allocate_state(s, n, neighborlist_capacity)) {
@@ -699,17 +709,18 @@ void md_enforce_pbc(void) {  // wraps locals only: a pending ghost carry stays p
     State& s = g_state;
     if (!require_alive("md_enforce_pbc")) return;
     flush_locals(s);
-    phase_mark(PH_OTHER);
-    run_enforce_pbc(s);
+    s.pend_pbc = true;  // held back for md_borders, which wraps in its first kernel
 }
 
 void md_borders(void) {
     State& s = g_state;
     if (!require_alive("md_borders")) return;
     s.pend_ghost = false;  // every ghost is written anew below: the carry would be overwritten
+    const bool wrap = s.pend_pbc;
+    s.pend_pbc = false;
     flush_all(s);
     phase_mark(PH_COMM);
-    run_borders(s);
+    run_borders(s, wrap);
 }
 
 void md_distribute_particles(void) {
@@ -752,6 +763,7 @@ void md_initial_integration(double dt) {
 void md_synchronize_ghost_layer(void) {
     State& s = g_state;
     if (!require_alive("md_synchronize_ghost_layer")) return;
+    flush_pbc(s);  // ghosts are refreshed from the wrapped locals
     flush_final(s);
     if (!s.pend_init) flush_kick(s);
     flush_force(s);
@@ -812,6 +824,7 @@ void md_compute_dem(bool half, double rc, double damping_n, double damping_t, do
 void md_final_integration(double dt) {
     State& s = g_state;
     if (!require_alive("md_final_integration")) return;
+    flush_pbc(s);
     flush_final(s);
     flush_ghost(s);
     flush_init(s);

@@ -80,9 +80,8 @@ __device__ __forceinline__ int rebase_cell(const double4& p, const GeoArgs& a) {
 // ---- periodic wrap ---------------------------------------------------------
 // comm/comm.impala:152-162: one wrap per axis with strict comparisons against
 // the world box.  img counts wraps so the adjoint can unwrap displacements.
-__global__ void k_enforce_pbc(double4* __restrict__ pos, int* __restrict__ img, int N, GeoArgs a) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+__device__ __forceinline__ double4 wrap_local(double4* __restrict__ pos, int* __restrict__ img, int i,
+                                              const GeoArgs& a) {
     double4 p = pos[i];
     double c[3] = {p.x, p.y, p.z};
     int im = img[i];
@@ -93,8 +92,16 @@ __global__ void k_enforce_pbc(double4* __restrict__ pos, int* __restrict__ img, 
         if (v < a.wlo[d]) { c[d] = dadd(c[d], a.len[d]); w[d] -= 1; }
         if (v > a.whi[d]) { c[d] = dsub(c[d], a.len[d]); w[d] += 1; }
     }
-    pos[i] = make_double4(c[0], c[1], c[2], p.w);
+    p = make_double4(c[0], c[1], c[2], p.w);
+    pos[i] = p;
     img[i] = pack3(w[0], w[1], w[2]);
+    return p;
+}
+
+__global__ void k_enforce_pbc(double4* __restrict__ pos, int* __restrict__ img, int N, GeoArgs a) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    wrap_local(pos, img, i, a);
 }
 
 // ---- borders ---------------------------------------------------------------
@@ -130,15 +137,22 @@ __device__ __forceinline__ unsigned border_mask(const double4& p, const GeoArgs&
     return mask | (flags << 26);
 }
 
-// Pass 1: masks in reference order and per-block per-type counts [26][nblk].
-__global__ void k_border_count(const double4* __restrict__ pos, const int* __restrict__ slot_of_ref,
-                               unsigned* __restrict__ bmask, int* __restrict__ bcount, int N, int nblk, GeoArgs a) {
+// Pass 1: masks in reference order and per-block per-type counts [26][nblk].  WRAP: the
+// periodic wrap of each local (k_enforce_pbc's) is done here first, one launch fewer.
+template <bool WRAP>
+__global__ void k_border_count(double4* __restrict__ pos, int* __restrict__ img, const int* __restrict__ slot_of_ref,
+                               unsigned* __restrict__ bmask, int* __restrict__ bcount, int N, int nblk, GeoArgs a,
+                               int* __restrict__ cnt, int nseg, DevStatus* st) {
     __shared__ int wc[8][26];
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // the binning that follows starts from zeroed cell counters and status (no memsets there)
+    for (int g = r; g < nseg; g += gridDim.x * blockDim.x) cnt[g] = 0;
+    if (r == 0) st->out_local = st->out_ghost = st->nchain = st->img_over1 = st->img_over2 = 0;
     unsigned m = 0;
     if (r < N) {
-        m = border_mask(pos[slot_of_ref[r]], a);
+        const int sl = slot_of_ref[r];
+        m = border_mask(WRAP ? wrap_local(pos, img, sl, a) : pos[sl], a);
         bmask[r] = m;
     }
     for (int t = 0; t < 26; ++t) {
@@ -291,8 +305,10 @@ __global__ void k_permute(const int* __restrict__ perm, const double4* __restric
                           int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rref,
                           int* __restrict__ rbk, const int* __restrict__ bin_cell, int* __restrict__ slot_cell,
                           float4* __restrict__ pos32, int* __restrict__ img_cnt, int* __restrict__ img_slot,
-                          int capA, int NA, int N, GeoArgs a, int mixed) {
+                          int capA, int NA, int N, GeoArgs a, int mixed, DevStatus* st) {
     int n = blockIdx.x * blockDim.x + threadIdx.x;
+    // the list build that follows starts from a zeroed status (no memset there)
+    if (n == 0) st->max_nb = st->bad_code = st->tile_overflow = st->halo_max = st->tile_blocks = 0;
     if (n >= NA) return;
     int o = perm[n];
     slot_cell[n] = bin_cell[o];
@@ -728,7 +744,7 @@ void run_enforce_pbc(State& s) {
 
 bool grow_atoms(State& s, int need);  // api.cu
 
-void run_borders(State& s) {
+void run_borders(State& s, bool wrap) {
     GeoArgs a = geo_args(s.geo);
     const int N = s.N;
     const int nblk = nblocks(N, 256);
@@ -737,7 +753,14 @@ void run_borders(State& s) {
         return;
     }
     prof_begin(K_BORDER);
-    k_border_count<<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.slot_of_ref, s.bmask, s.bcount, N, nblk, a);
+    const int nseg = 2 * (a.ncells + 1);
+    if (wrap)
+        k_border_count<true><<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
+                                                          s.bcount, N, nblk, a, s.cnt, nseg, s.status_dev);
+    else
+        k_border_count<false><<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
+                                                           s.bcount, N, nblk, a, s.cnt, nseg, s.status_dev);
+    s.bin_zeroed = true;
     launched(K_BORDER);
     const int n = 26 * nblk;
     // boff = exclusive scan of bcount, stored after the counts
@@ -783,8 +806,11 @@ void run_distribute(State& s) {
     const int nseg = 2 * (a.ncells + 1);
     if (NA == 0) return;
     prof_begin(K_BIN);
-    TMD_CUDA(cudaMemsetAsync(s.cnt, 0, sizeof(int) * nseg, s.stream));
-    TMD_CUDA(cudaMemsetAsync(&s.status_dev->out_local, 0, 5 * sizeof(int), s.stream));  // .. img_over2
+    if (!s.bin_zeroed) {  // else zeroed by the border pass's first kernel
+        TMD_CUDA(cudaMemsetAsync(s.cnt, 0, sizeof(int) * nseg, s.stream));
+        TMD_CUDA(cudaMemsetAsync(&s.status_dev->out_local, 0, 5 * sizeof(int), s.stream));  // .. img_over2
+    }
+    s.bin_zeroed = false;
     k_bin_count<<<nblocks(NA, 256), 256, 0, s.stream>>>(s.pos.b[s.pc], s.cnt, s.bin_cell, s.bin_rank, s.status_dev,
                                                         N, NA, a);
     launched(K_BIN);
@@ -799,8 +825,9 @@ void run_distribute(State& s) {
     k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
         s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
         s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk,
-        s.bin_cell, s.slot_cell, s.pos32.b[np], s.img_cnt, s.img_slot, s.capA, NA, N, a, s.precision);
+        s.bin_cell, s.slot_cell, s.pos32.b[np], s.img_cnt, s.img_slot, s.capA, NA, N, a, s.precision, s.status_dev);
     launched(K_BIN);
+    s.build_zeroed = true;
     s.pc = np;
     s.vc = nv;
     s.ac = na;
@@ -845,7 +872,9 @@ int run_build_lists(State& s, bool half, double cutoff) {
         a.nxy = g.nx * g.ny;
         for (int d = 0; d < 3; ++d) a.alo[d] = g.aabb_lo[d];
         a.spacing = g.spacing;
-        TMD_CUDA(cudaMemsetAsync(&s.status_dev->max_nb, 0, 5 * sizeof(int), s.stream));  // .. tile_blocks
+        if (attempt > 0 || !s.build_zeroed)  // else zeroed by the binning's reorder kernel
+            TMD_CUDA(cudaMemsetAsync(&s.status_dev->max_nb, 0, 5 * sizeof(int), s.stream));  // .. tile_blocks
+        s.build_zeroed = false;
         prof_begin(K_NLIST);
         const int nb = nblocks(g.ncells, kNlWarps);
         // the tiled builder declines when its shared-memory need (halo capacity and

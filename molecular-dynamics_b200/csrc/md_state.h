@@ -227,6 +227,13 @@ struct State {
     PendingForce final_cfg;
     // locals were integrated by that fused kernel; ghosts still to be refreshed or carried
     bool pend_ghost = false;
+    // md_enforce_pbc held back: md_borders does the wrap in its first kernel, any other call
+    // launches it alone
+    bool pend_pbc = false;
+    // the cell counters and binning status were zeroed by the last border pass (cleared by
+    // the binning that uses them)
+    bool bin_zeroed = false;
+    bool build_zeroed = false;  // likewise the list-build status, by the binning's reorder kernel
 
     // reported iteration counters (core/runtime.impala:3-5)
     long long force_iters = 0, rsq_iters = 0, integration_iters = 0;
@@ -259,7 +266,7 @@ void prof_reset();
 // ---- kernels (launch wrappers, all on g_state.stream) ---------------------
 struct KLaunch;  // fwd
 void run_enforce_pbc(State& s);
-void run_borders(State& s);                       // ghost generation, reference order
+void run_borders(State& s, bool wrap = false);   // ghost generation, reference order (wrap: the periodic wrap first)
 void run_distribute(State& s);                    // binning + reorder
 int run_build_lists(State& s, bool half, double cutoff);  // returns 0 or error
 // tiled full-list build (k_tile.cu): 1 = built, 0 = not applicable (caller builds
