@@ -230,7 +230,7 @@ std::vector<SlabItem> slab_items(State& s) {
     int** keep[] = {&s.rbk, &s.slot_of_ref, &s.rref, &s.gsrc, &s.groot, &s.gcode, &s.bsrc_ref, &s.broot_ref,
                     &s.bcode};
     for (int** q : keep) v.push_back(item(q, 1, true));
-    int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.perm, &s.nbn, &s.slot_cell, &s.chain};
+    int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.nbn, &s.slot_cell, &s.chain};
     for (int** q : scratch) v.push_back(item(q, 1, false));
     v.push_back(item(&s.img_cnt, 2, false));
     v.push_back(item(&s.img_slot, kImgW, false));

@@ -276,66 +276,72 @@ __global__ void k_bin_scatter(const int* __restrict__ ref, const int* __restrict
     tmp_src[p] = s;
 }
 
-// One warp per segment: rank members by reference index (keys are unique).
-// The two outside-the-grid buckets keep arrival order: their members have no
-// neighbours and are nobody's neighbour, so their order is not observable.
-__global__ void k_bin_rank(const int* __restrict__ cstart, const int* __restrict__ tmp_key,
-                           const int* __restrict__ tmp_src, int* __restrict__ perm, int nseg, int ncells) {
-    int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (w >= nseg) return;
-    int a = cstart[w], b = cstart[w + 1];
-    if (w == ncells || w == 2 * ncells + 1) {
-        for (int e = a + lane; e < b; e += 32) perm[e] = tmp_src[e];
-        return;
+// One warp per segment: rank the members by reference index (keys are unique) and move
+// each one from its old slot to its new one (cstart[segment] + rank).  The two outside-
+// the-grid buckets keep arrival order: their members have no neighbours and are nobody's
+// neighbour, so their order is not observable.
+struct MoveArgs {
+    const double4* pos_o; double4* pos_n;
+    const double4* vel_o; double4* vel_n;
+    const double4* frc_o; double4* frc_n;
+    const double* mass_o; double* mass_n;
+    const int* ref_o; int* ref_n;
+    const int* img_o; int* img_n;
+    int* slot_of_ref; int* rref; int* rbk;
+    const int* bin_cell; int* slot_cell;
+    float4* pos32; int* img_cnt; int* img_slot;
+    int capA, N, mixed;
+};
+
+__device__ __forceinline__ void move_slot(int n, int o, const MoveArgs& m, const GeoArgs& a) {
+    m.slot_cell[n] = m.bin_cell[o];
+    const double4 p = m.pos_o[o];
+    m.pos_n[n] = p;
+    m.vel_n[n] = m.vel_o[o];
+    m.frc_n[n] = m.frc_o[o];
+    m.mass_n[n] = m.mass_o[o];
+    const int r = m.ref_o[o];
+    m.ref_n[n] = r;
+    if (n < m.N) {
+        m.img_n[n] = m.img_o[o];
+        m.rref[n] = r;
+        // empty image records for k_ghost_links to fill
+        m.img_cnt[n] = 0;
+        m.img_cnt[m.capA + n] = 0;
+#pragma unroll
+        for (int k = 0; k < kImgW; ++k) m.img_slot[(size_t)k * m.capA + n] = -1;
     }
-    for (int e = a + lane; e < b; e += 32) {
-        int key = tmp_key[e];
-        int rank = 0;
-        for (int f = a; f < b; ++f) rank += tmp_key[f] < key;
-        perm[a + rank] = tmp_src[e];
-    }
+    m.slot_of_ref[r] = n;
+    const int k = rebase_cell(p, a);
+    m.rbk[n] = k;
+    if (m.mixed) m.pos32[n] = rebased32(p, k, a.alo, a.rb_h);
 }
 
-__global__ void k_permute(const int* __restrict__ perm, const double4* __restrict__ pos_o, double4* __restrict__ pos_n,
-                          const double4* __restrict__ vel_o, double4* __restrict__ vel_n,
-                          const double4* __restrict__ frc_o, double4* __restrict__ frc_n,
-                          const double* __restrict__ mass_o, double* __restrict__ mass_n,
-                          const int* __restrict__ ref_o, int* __restrict__ ref_n, const int* __restrict__ img_o,
-                          int* __restrict__ img_n, int* __restrict__ slot_of_ref, int* __restrict__ rref,
-                          int* __restrict__ rbk, const int* __restrict__ bin_cell, int* __restrict__ slot_cell,
-                          float4* __restrict__ pos32, int* __restrict__ img_cnt, int* __restrict__ img_slot,
-                          int capA, int NA, int N, GeoArgs a, int mixed, DevStatus* st) {
-    int n = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_rank_move(const int* __restrict__ cstart, const int* __restrict__ tmp_key,
+                            const int* __restrict__ tmp_src, int nseg, int ncells, MoveArgs m, GeoArgs ga,
+                            DevStatus* st) {
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     // the list build that follows starts from a zeroed status (no memset there)
-    if (n == 0) st->max_nb = st->bad_code = st->tile_overflow = st->halo_max = st->tile_blocks = 0;
-    if (n >= NA) return;
-    int o = perm[n];
-    slot_cell[n] = bin_cell[o];
-    double4 p = pos_o[o];
-    pos_n[n] = p;
-    vel_n[n] = vel_o[o];
-    frc_n[n] = frc_o[o];
-    mass_n[n] = mass_o[o];
-    int r = ref_o[o];
-    ref_n[n] = r;
-    if (n < N) {
-        img_n[n] = img_o[o];
-        rref[n] = r;
-        // empty image records for k_ghost_links to fill
-        img_cnt[n] = 0;
-        img_cnt[capA + n] = 0;
-#pragma unroll
-        for (int k = 0; k < kImgW; ++k) img_slot[(size_t)k * capA + n] = -1;
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        st->max_nb = st->bad_code = st->tile_overflow = st->halo_max = st->tile_blocks = 0;
+    if (gw >= nseg) return;
+    const int a = cstart[gw], b = cstart[gw + 1];
+    const bool outside = gw == ncells || gw == 2 * ncells + 1;
+    for (int e = a + lane; e < b; e += 32) {
+        int n = e;
+        if (!outside) {
+            const int key = tmp_key[e];
+            int rank = 0;
+            for (int f = a; f < b; ++f) rank += tmp_key[f] < key;
+            n = a + rank;
+        }
+        move_slot(n, tmp_src[e], m, ga);
     }
-    slot_of_ref[r] = n;
-    int k = rebase_cell(p, a);
-    rbk[n] = k;
-    if (mixed) pos32[n] = rebased32(p, k, a.alo, a.rb_h);
 }
 
 // Per ghost: its source, root and shift code in slot terms, and its place in the image
-// records of the locals (k_permute emptied them): a local's direct two-phase images (ghosts
+// records of the locals (k_rank_move emptied them): a local's direct two-phase images (ghosts
 // whose source it is) and all its images (ghosts whose root it is), one plane per image
 // number (filled in order, -1 beyond the last); ghosts whose two-phase source is another
 // ghost go to `chain`.  The order within a record follows the atomics, but every ghost is
@@ -818,14 +824,20 @@ void run_distribute(State& s) {
     k_bin_scatter<<<nblocks(NA, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.bin_cell, s.bin_rank, s.cstart,
                                                           s.tmp_key, s.tmp_src, N, NA, a.ncells);
     launched(K_BIN);
-    k_bin_rank<<<nblocks((long long)nseg * 32, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, s.perm,
-                                                                          nseg, a.ncells);
-    launched(K_BIN);
     const int np = 1 - s.pc, nv = 1 - s.vc, na = 1 - s.ac;
-    k_permute<<<nblocks(NA, 256), 256, 0, s.stream>>>(
-        s.perm, s.pos.b[s.pc], s.pos.b[np], s.vel.b[s.vc], s.vel.b[nv], s.frc.b[s.ac], s.frc.b[na], s.mass.b[s.ac],
-        s.mass.b[na], s.ref.b[s.ac], s.ref.b[na], s.img.b[s.ac], s.img.b[na], s.slot_of_ref, s.rref, s.rbk,
-        s.bin_cell, s.slot_cell, s.pos32.b[np], s.img_cnt, s.img_slot, s.capA, NA, N, a, s.precision, s.status_dev);
+    MoveArgs m;
+    m.pos_o = s.pos.b[s.pc]; m.pos_n = s.pos.b[np];
+    m.vel_o = s.vel.b[s.vc]; m.vel_n = s.vel.b[nv];
+    m.frc_o = s.frc.b[s.ac]; m.frc_n = s.frc.b[na];
+    m.mass_o = s.mass.b[s.ac]; m.mass_n = s.mass.b[na];
+    m.ref_o = s.ref.b[s.ac]; m.ref_n = s.ref.b[na];
+    m.img_o = s.img.b[s.ac]; m.img_n = s.img.b[na];
+    m.slot_of_ref = s.slot_of_ref; m.rref = s.rref; m.rbk = s.rbk;
+    m.bin_cell = s.bin_cell; m.slot_cell = s.slot_cell;
+    m.pos32 = s.pos32.b[np]; m.img_cnt = s.img_cnt; m.img_slot = s.img_slot;
+    m.capA = s.capA; m.N = N; m.mixed = s.precision;
+    k_rank_move<<<nblocks((long long)nseg * 32, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, nseg,
+                                                                           a.ncells, m, a, s.status_dev);
     launched(K_BIN);
     s.build_zeroed = true;
     s.pc = np;

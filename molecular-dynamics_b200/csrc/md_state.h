@@ -166,7 +166,6 @@ struct State {
     int* bin_rank = nullptr;   // per slot: arrival rank within its cell
     int* tmp_key = nullptr;    // per sorted position: reference index
     int* tmp_src = nullptr;    // per sorted position: old slot
-    int* perm = nullptr;       // new slot -> old slot
     int* slot_cell = nullptr;  // per (sorted) slot: its cell, ncells when outside the grid
     // ghost images by local (k_ghost_links at every distribution): the force kernel that does
     // the next initial integration writes them, so no separate ghost refresh is needed
