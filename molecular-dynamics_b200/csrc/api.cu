@@ -400,6 +400,7 @@ void flush_pbc(State& s) {
 }
 
 void flush_all(State& s) {
+    flush_links(s);
     flush_final(s);
     flush_ghost(s);
     flush_init(s);
@@ -411,6 +412,7 @@ void flush_all(State& s) {
 // everything but the carried-over ghosts: for calls that touch only the locals, so that a
 // following md_borders, which writes every ghost anew, can drop the carry
 void flush_locals(State& s) {
+    flush_links(s);
     flush_final(s);
     flush_init(s);
     flush_kick(s);
@@ -605,7 +607,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.pend_init = false;
     s.pend_force = PendingForce();
     s.pend_final = s.pend_ghost = s.pend_kick = s.pend_pbc = false;
-    s.bin_zeroed = s.build_zeroed = false;
+    s.bin_zeroed = s.build_zeroed = s.pend_links = false;
     s.force_iters = s.rsq_iters = s.integration_iters = 0;
     s.launches = 0;
     if (!allocate_state(s, n, neighborlist_capacity)) {
@@ -734,7 +736,12 @@ void md_distribute_particles(void) {
 void md_assemble_neighborlists(bool half, double cutoff) {
     State& s = g_state;
     if (!require_alive("md_assemble_neighborlists")) return;
+    // pending ghost links stay pending: the list build runs them as extra blocks (nothing
+    // else is pending after md_distribute_particles, which set them last)
+    const bool links = s.pend_links;
+    s.pend_links = false;
     flush_all(s);
+    s.pend_links = links;
     phase_mark(PH_NEIGH);
     run_build_lists(s, half, cutoff);
 }
@@ -763,6 +770,7 @@ void md_initial_integration(double dt) {
 void md_synchronize_ghost_layer(void) {
     State& s = g_state;
     if (!require_alive("md_synchronize_ghost_layer")) return;
+    flush_links(s);
     flush_pbc(s);  // ghosts are refreshed from the wrapped locals
     flush_final(s);
     if (!s.pend_init) flush_kick(s);
@@ -824,6 +832,7 @@ void md_compute_dem(bool half, double rc, double damping_n, double damping_t, do
 void md_final_integration(double dt) {
     State& s = g_state;
     if (!require_alive("md_final_integration")) return;
+    flush_links(s);
     flush_pbc(s);
     flush_final(s);
     flush_ghost(s);

@@ -346,32 +346,38 @@ __global__ void k_rank_move(const int* __restrict__ cstart, const int* __restric
 // number (filled in order, -1 beyond the last); ghosts whose two-phase source is another
 // ghost go to `chain`.  The order within a record follows the atomics, but every ghost is
 // written exactly once, so the result is deterministic.
-__global__ void k_ghost_links(const int* __restrict__ ref, const int* __restrict__ slot_of_ref,
-                              const int* __restrict__ bsrc_ref, const int* __restrict__ broot_ref,
-                              const int* __restrict__ bcode, int* __restrict__ gsrc, int* __restrict__ groot,
-                              int* __restrict__ gcode, int* __restrict__ rref, int* __restrict__ img_cnt,
-                              int* __restrict__ img_slot, int* __restrict__ chain, DevStatus* st, int N, int G,
-                              int capA) {
-    int h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= G) return;
-    int g = ref[N + h] - N;
-    const int s1 = slot_of_ref[bsrc_ref[g]];
-    const int r = slot_of_ref[broot_ref[g]];
-    gsrc[h] = s1;
-    groot[h] = r;
-    gcode[h] = bcode[g];
-    rref[N + h] = broot_ref[g];
+struct LinkArgs {
+    const int* ref; const int* slot_of_ref; const int* bsrc_ref; const int* broot_ref; const int* bcode;
+    int* gsrc; int* groot; int* gcode; int* rref; int* img_cnt; int* img_slot; int* chain;
+    DevStatus* st;
+    int N, G, capA;
+};
+
+__device__ __forceinline__ void ghost_link(int h, const LinkArgs& l) {
+    const int N = l.N, capA = l.capA;
+    int g = l.ref[N + h] - N;
+    const int s1 = l.slot_of_ref[l.bsrc_ref[g]];
+    const int r = l.slot_of_ref[l.broot_ref[g]];
+    l.gsrc[h] = s1;
+    l.groot[h] = r;
+    l.gcode[h] = l.bcode[g];
+    l.rref[N + h] = l.broot_ref[g];
     const int t = N + h;
     if (s1 < N) {
-        const int k = atomicAdd(&img_cnt[s1], 1);
-        if (k < kImg1) img_slot[(size_t)k * capA + s1] = t;
-        else atomicAdd(&st->img_over1, 1);
+        const int k = atomicAdd(&l.img_cnt[s1], 1);
+        if (k < kImg1) l.img_slot[(size_t)k * capA + s1] = t;
+        else atomicAdd(&l.st->img_over1, 1);
     } else {
-        chain[atomicAdd(&st->nchain, 1)] = h;
+        l.chain[atomicAdd(&l.st->nchain, 1)] = h;
     }
-    const int k2 = atomicAdd(&img_cnt[capA + r], 1);
-    if (k2 < kImg2) img_slot[(size_t)(kImg1 + k2) * capA + r] = t;
-    else atomicAdd(&st->img_over2, 1);
+    const int k2 = atomicAdd(&l.img_cnt[capA + r], 1);
+    if (k2 < kImg2) l.img_slot[(size_t)(kImg1 + k2) * capA + r] = t;
+    else atomicAdd(&l.st->img_over2, 1);
+}
+
+__global__ void k_ghost_links(LinkArgs l) {
+    const int h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h < l.G) ghost_link(h, l);
 }
 
 // ---- neighbour lists ---------------------------------------------------------
@@ -417,13 +423,18 @@ template <int HM>
 __global__ void __launch_bounds__(kNlWarps * 32, TMD_NL_MINB)
 k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
              const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl, DevStatus* st,
-             NlArgs a) {
+             NlArgs a, int cell_blocks, LinkArgs la) {
     __shared__ float4 s_cpos[kNlWarps][kNlTile];  // kept candidate position (cell-centre relative), w = slot << 6
     __shared__ int s_crel[kNlWarps][kNlTile];     // its rebasing cell relative to the first home's
     __shared__ int s_cref[kNlWarps][HM ? kNlTile : 1];
     __shared__ int s_rstart[kNlWarps][54];
     __shared__ int s_rpre[kNlWarps][55];
 
+    if (blockIdx.x >= cell_blocks) {  // blocks past the cells link the ghosts (k_ghost_links' work)
+        const int h = (blockIdx.x - cell_blocks) * blockDim.x + threadIdx.x;
+        if (h < la.G) ghost_link(h, la);
+        return;
+    }
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * kNlWarps + wid;
     if (c >= a.ncells) return;
@@ -843,12 +854,9 @@ void run_distribute(State& s) {
     s.pc = np;
     s.vc = nv;
     s.ac = na;
-    if (s.G > 0) {
-        k_ghost_links<<<nblocks(s.G, 256), 256, 0, s.stream>>>(s.ref.b[s.ac], s.slot_of_ref, s.bsrc_ref, s.broot_ref,
-                                                               s.bcode, s.gsrc, s.groot, s.gcode, s.rref, s.img_cnt,
-                                                               s.img_slot, s.chain, s.status_dev, N, s.G, s.capA);
-        launched(K_BIN);
-    }
+    // the ghost links run as extra blocks of the list build that follows, or alone
+    // (flush_links) before anything else that reads them
+    s.pend_links = s.G > 0;
     s.img_ok = 0;  // known after the status readback of the list build
     s.nchain = 0;
     prof_end(K_BIN);
@@ -857,6 +865,34 @@ void run_distribute(State& s) {
 }
 
 void grow_lists(State& s, int rows);  // api.cu
+
+LinkArgs link_args(State& s) {
+    LinkArgs l;
+    l.ref = s.ref.b[s.ac];
+    l.slot_of_ref = s.slot_of_ref;
+    l.bsrc_ref = s.bsrc_ref;
+    l.broot_ref = s.broot_ref;
+    l.bcode = s.bcode;
+    l.gsrc = s.gsrc;
+    l.groot = s.groot;
+    l.gcode = s.gcode;
+    l.rref = s.rref;
+    l.img_cnt = s.img_cnt;
+    l.img_slot = s.img_slot;
+    l.chain = s.chain;
+    l.st = s.status_dev;
+    l.N = s.N;
+    l.G = s.G;
+    l.capA = s.capA;
+    return l;
+}
+
+void flush_links(State& s) {
+    if (!s.pend_links) return;
+    s.pend_links = false;
+    k_ghost_links<<<nblocks(s.G, 256), 256, 0, s.stream>>>(link_args(s));
+    launched(K_BIN);
+}
 
 int run_build_lists(State& s, bool half, double cutoff) {
     const Geometry& g = s.geo;
@@ -870,6 +906,9 @@ int run_build_lists(State& s, bool half, double cutoff) {
     // sends the whole build back to k_build_list
     bool use_tiles = !half && tiles_usable(s);
     s.tiles_valid = 0;
+    // the half lists that keep boundary pairs read the ghosts' root references, which the
+    // links write; the tiled builder takes no link blocks
+    if (use_tiles || (half && s.half_ghost)) flush_links(s);
     for (int attempt = 0; attempt < 8; ++attempt) {
         NlArgs a;
         a.cut2 = cutoff * cutoff;
@@ -893,15 +932,21 @@ int run_build_lists(State& s, bool half, double cutoff) {
         // list capacity, both of which grow between attempts) exceeds the limit
         if (use_tiles && run_build_tiles(s, cutoff) != 1) use_tiles = false;
         if (!use_tiles) {
+            // the pending ghost links ride along as extra blocks (once: they count with atomics)
+            const LinkArgs la = link_args(s);
+            const int lb = s.pend_links ? nblocks(s.G, kNlWarps * 32) : 0;
+            s.pend_links = false;
             if (half && s.half_ghost)
-                k_build_list<2><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart,
-                                                                        s.nbn, s.nbl, s.status_dev, a);
+                k_build_list<2><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart,
+                                                                         s.nbn, s.nbl, s.status_dev, a, nb, la);
             else if (half)
-                k_build_list<1><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk,
-                                                                        s.cstart, s.nbn, s.nbl, s.status_dev, a);
+                k_build_list<1><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk,
+                                                                         s.cstart, s.nbn, s.nbl, s.status_dev, a, nb,
+                                                                         la);
             else
-                k_build_list<0><<<nb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk,
-                                                                        s.cstart, s.nbn, s.nbl, s.status_dev, a);
+                k_build_list<0><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk,
+                                                                         s.cstart, s.nbn, s.nbl, s.status_dev, a, nb,
+                                                                         la);
         }
         launched(K_NLIST);
         prof_end(K_NLIST);

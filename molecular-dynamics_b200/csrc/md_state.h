@@ -233,6 +233,7 @@ struct State {
     // the binning that uses them)
     bool bin_zeroed = false;
     bool build_zeroed = false;  // likewise the list-build status, by the binning's reorder kernel
+    bool pend_links = false;    // ghost links of the last binning not yet launched (see flush_links)
 
     // reported iteration counters (core/runtime.impala:3-5)
     long long force_iters = 0, rsq_iters = 0, integration_iters = 0;
@@ -265,6 +266,7 @@ void prof_reset();
 // ---- kernels (launch wrappers, all on g_state.stream) ---------------------
 struct KLaunch;  // fwd
 void run_enforce_pbc(State& s);
+void flush_links(State& s);                      // the deferred ghost links of a binning, if pending
 void run_borders(State& s, bool wrap = false);   // ghost generation, reference order (wrap: the periodic wrap first)
 void run_distribute(State& s);                    // binning + reorder
 int run_build_lists(State& s, bool half, double cutoff);  // returns 0 or error
