@@ -175,21 +175,65 @@ def replica_rate(atoms_per_rank, world, steps, ms_local, dist, device=None):
 
 
 # ---------------------------------------------------------------------------
-def cpu_run(steps, threads, cells=CELLS, warmup=1):
-    """The oracle's CPU path on `threads` host threads; returns (atom-steps/s, atoms, seconds)."""
+def cpu_info():
+    """CPU model, the AVX-512 feature flags and the host threads of this machine."""
+    model, flags = None, []
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if model is None and line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                if not flags and line.startswith("flags"):
+                    flags = sorted(x for x in line.split(":", 1)[1].split() if x.startswith("avx512"))
+    except OSError:
+        pass
+    return {"model": model, "avx512_flags": flags, "threads": os.cpu_count()}
+
+
+_native_oracle = None
+
+
+def native_oracle():
+    """The oracle compiled on this host with -march=native (make -C oracle native, always remade
+    here so a copy built on another machine is never timed); falls back to the portable build."""
+    global _native_oracle
+    if _native_oracle is None:
+        r = subprocess.run(["make", "-B", "-C", os.path.join(ROOT, "oracle"), "native"], capture_output=True)
+        if r.returncode == 0:
+            _native_oracle = (os.path.join(ROOT, "oracle", "_build_native", "libtinymd_oracle.so"), "-O3 -march=native")
+        else:
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
+            _native_oracle = (os.path.join(ROOT, "oracle", "_build", "libtinymd_oracle.so"),
+                              "-O3 -march=x86-64-v3 (native build failed)")
+    return _native_oracle
+
+
+def cpu_lattice(cells=CELLS):
+    """The workload's lattice from the reference's own generator (oracle/_ref), so the CPU arm
+    loads no product code; the product's identical generator only where oracle/_ref is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_lattice
+    if ref_lattice.available():
+        return ref_lattice.reference_lattice(cells), "reference initialize.h (oracle/_ref)"
     import tinymd
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True, capture_output=True)
-    ora = tinymd.open_library(os.path.join(ROOT, "oracle", "_build", "libtinymd_oracle.so"))
+    return tinymd.setup_particles("default", cells, lib=tinymd.load()), "product setups (oracle/_ref not built)"
+
+
+def cpu_run(steps, threads, cells=CELLS, warmup=1):
+    """The oracle's CPU path on `threads` host threads; returns (atom-steps/s, atoms, seconds, notes)."""
+    import tinymd
+    path, flags = native_oracle()
+    ora = tinymd.open_library(path)
     ora.oracle_set_threads(threads)
-    setup_lib = tinymd.load(build_if_missing=True)
-    m, x, v, world, rank = tinymd.setup_particles("default", cells, lib=setup_lib)
+    (m, x, v, world, rank), source = cpu_lattice(cells)
     sim = tinymd.Simulation(ora, m, x, v, world, rank, temp=1.44)
     sim.step(DT, warmup)
     t0 = time.perf_counter()
     sim.step(DT, steps)
     t = time.perf_counter() - t0
     sim.close()
-    return len(m) * steps / t, len(m), t
+    notes = {"build": flags, "lattice": source, "cpu": cpu_info()}
+    return len(m) * steps / t, len(m), t, notes
 
 
 def run_reference(args):
@@ -198,7 +242,7 @@ def run_reference(args):
         return 0
     threads = os.cpu_count() or 1
     steps = args.steps
-    rate, natoms, secs = cpu_run(steps, threads, warmup=min(args.warmup, 20))
+    rate, natoms, secs, notes = cpu_run(steps, threads, warmup=min(args.warmup, 20))
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / steps, "higher_is_better": True, "scaling": "weak",
@@ -206,7 +250,8 @@ def run_reference(args):
         "config": {"workload": "lj_default_fcc_32x32x32_131072_atoms_full_list", "atoms": natoms, "dt": DT,
                    "reneigh": 20, "cutoff": 2.5, "skin": 0.3},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{natoms} atoms x {steps} timesteps (full workload), OpenMP over atoms"},
+                         "sample": f"{natoms} atoms x {steps} timesteps (full workload), OpenMP over atoms",
+                         **notes},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -502,11 +547,11 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         steps = 40
-        rate, n_cpu, secs = cpu_run(steps, threads)
+        rate, n_cpu, secs, notes = cpu_run(steps, threads)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{n_cpu} atoms x {steps} timesteps of the same workload"}
+                                "sample": f"{n_cpu} atoms x {steps} timesteps of the same workload", **notes}
         # one thread: what the reference's cpu backend does (its -t flag is only printed)
-        rate1, _, _ = cpu_run(10, 1)
+        rate1, _, _, _ = cpu_run(10, 1)
         line["cpu_baseline_1thread"] = {"value": rate1, "unit": UNIT, "cores": 1, "kind": "port",
                                         "sample": f"{n_cpu} atoms x 10 timesteps of the same workload"}
     if dist is not None:

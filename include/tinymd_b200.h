@@ -61,21 +61,21 @@ void md_rescale_grid(double const *aabb);
 void md_copy_data_from_accelerator(void);
 /* anydsl_includes.h:13, core/grid.impala:360-367 (host mirror -> device) */
 void md_copy_data_to_accelerator(void);
-/* anydsl_includes.h:14, core/compute.impala:175-184: v += dt/2 f; x += dt v */
+/* anydsl_includes.h:14, core/compute.impala:97-106: v += dt/2 f; x += dt v */
 void md_initial_integration(double dt);
-/* anydsl_includes.h:15, core/compute.impala:186-194: v += dt/2 f */
+/* anydsl_includes.h:15, core/compute.impala:108-116: v += dt/2 f */
 void md_final_integration(double dt);
-/* anydsl_includes.h:16, core/compute.impala:196-200 (single periodic wrap of locals) */
+/* anydsl_includes.h:16, core/compute.impala:118-122 (single periodic wrap of locals) */
 void md_enforce_pbc(void);
-/* anydsl_includes.h:17, core/grid.impala:497-513: copies the host mirror of the
+/* anydsl_includes.h:17, core/grid.impala:483-499: copies the host mirror of the
  * locals, in input order; returns the number of locals. */
 int md_write_grid_data_to_arrays(double *masses, struct Vector3D *positions, struct Vector3D *velocities,
                                  struct Vector3D *forces);
-/* anydsl_includes.h:18, core/grid.impala:515-532: ghosts in the reference's
+/* anydsl_includes.h:18, core/grid.impala:501-518: ghosts in the reference's
  * ghost order; returns the number of LOCALS, as the reference does. */
 int md_write_grid_ghost_data_to_arrays(double *masses, struct Vector3D *positions, struct Vector3D *velocities,
                                        struct Vector3D *forces);
-/* anydsl_includes.h:19, core/grid.impala:534-560: the 8 grid box corners */
+/* anydsl_includes.h:19, core/grid.impala:520-546: the 8 grid box corners */
 int md_write_grid_aabb_data_to_arrays(double *masses, struct Vector3D *positions, struct Vector3D *velocities,
                                       struct Vector3D *forces);
 /* anydsl_includes.h:20, core/grid.impala:323-358: bins locals and ghosts into
@@ -159,21 +159,6 @@ void md_set_ghost_mode(int exact);
  * pairs are kept when the ghost's root local precedes i, and the reaction
  * force goes to that root. */
 void md_set_half_mode(int ghost_pairs);
-/* Tiled full lists (default 0): full-list builds run one block per row
- * segment of cells and also write per-warp streams of 16-bit halo indices
- * that the mixed form's force kernel walks against shared-memory staged
- * positions.  The lists are the same entry for entry; the staged kernel's
- * forces differ from the plain-list kernel's by FP32 summation order only.
- * On B200 this path is measured slower than the default per-cell builder and
- * plain-list kernel, so it is opt-in. */
-void md_set_tile_mode(int enable);
-/* 1 when the current full lists were built by the tiled builder (the mixed
- * form's force then runs the staged kernel), else 0. */
-int md_tiles_active(void);
-/* out[6] = {tiled lists active, builder halo capacity, largest staged halo of the
- * current lists, list capacity, blocks the last tiled build could not take,
- * largest halo seen by the last tiled build}. */
-void md_tile_info(int *out);
 /* DEM contact model: 0 = the reference closure (its contact branch is
  * unreachable, so the force is zero; default), 1 = contact-fixed
  * spring-dashpot with contact radius `radius` (overlap 2R - r > 0). */
@@ -235,8 +220,10 @@ int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double 
  * out, sums [4] out = {sum of 4 eps (s12 - s6), sum of f r^2, pairs inside the
  * cutoff, 0} over the list entries.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress) and should therefore come
- * before any stream capture.  Calls share the array: calls that overlap on
- * the GPU race.  Returns MD_OK or an md_error code. */
+ * before any stream capture; that address is kept for the life of the
+ * process, so after a device reset the library must be loaded again.  Calls
+ * share the array: calls that overlap on the GPU race.  Returns MD_OK or an
+ * md_error code. */
 int md_lj_forces_noalloc(const double *positions, int n_local, const int *list_sizes, const int *lists, int stride,
                          int max_neighbors, double cutoff, double epsilon, double sigma, double *forces, double *sums,
                          void *stream);

@@ -27,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC, "-I" + HOST]
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + INC, "-I" + HOST]
 
-CU_SOURCES = ["api.cu", "k_neigh.cu", "k_step.cu", "k_tile.cu", "adjoint.cu", "noalloc.cu"]
+CU_SOURCES = ["api.cu", "k_neigh.cu", "k_step.cu", "adjoint.cu", "noalloc.cu"]
 CPP_LIB_SOURCES = [os.path.join(CSRC, "setup_api.cpp"), os.path.join(HOST, "setups.cpp")]
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] + \
           [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")] + \

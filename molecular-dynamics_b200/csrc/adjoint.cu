@@ -110,8 +110,8 @@ k_adj_hvp_split(const double4* __restrict__ xs, const double4* __restrict__ w, d
 #pragma unroll
         for (int b = 0; b < kHb; ++b) {
             const int k = sub + b * kLpa;
-            ej[b] = k < n ? (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits) : i;
-            er[b] = k < n ? __ldg(nbr + (size_t)k * a.stride + i) : i;
+            ej[b] = k < n ? (int)(__ldg(nbl + nl_index(k, i, a.stride)) >> kCodeBits) : i;
+            er[b] = k < n ? __ldg(nbr + nl_index(k, i, a.stride)) : i;
         }
         for (int k0 = sub; k0 < n; k0 += kLpa * kHb) {
             double4 xj[kHb], wj[kHb];
@@ -123,8 +123,8 @@ k_adj_hvp_split(const double4* __restrict__ xs, const double4* __restrict__ w, d
 #pragma unroll
             for (int b = 0; b < kHb; ++b) {
                 const int k = k0 + kLpa * kHb + b * kLpa;
-                ej[b] = k < n ? (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits) : i;
-                er[b] = k < n ? __ldg(nbr + (size_t)k * a.stride + i) : i;
+                ej[b] = k < n ? (int)(__ldg(nbl + nl_index(k, i, a.stride)) >> kCodeBits) : i;
+                er[b] = k < n ? __ldg(nbr + nl_index(k, i, a.stride)) : i;
             }
 #pragma unroll
             for (int b = 0; b < kHb; ++b) {
@@ -184,8 +184,8 @@ __global__ void k_root_list(const int* __restrict__ nbn, const uint32_t* __restr
     if (i >= N) return;
     const int n = min(nbn[i], nbcap);
     for (int k = 0; k < n; ++k) {
-        const int j = (int)(nbl[(size_t)k * stride + i] >> kCodeBits);
-        nbr[(size_t)k * stride + i] = j < N ? j : groot[j - N];
+        const int j = (int)(nbl[nl_index(k, i, stride)] >> kCodeBits);
+        nbr[nl_index(k, i, stride)] = j < N ? j : groot[j - N];
     }
 }
 
@@ -223,7 +223,7 @@ k_adj_init(const double4* __restrict__ pos, const int* __restrict__ img, const i
         av[i] = make_double4(dt * a.x, dt * a.y, dt * a.z, 0.0);
         const int n = min(nbn[i], nbcap);
         for (int k = 0; k < n; ++k) {
-            const int j = (int)(__ldg(nbl + (size_t)k * stride + i) >> kCodeBits);
+            const int j = (int)(__ldg(nbl + nl_index(k, i, stride)) >> kCodeBits);
             const double4 q = pos[j];
             const double dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
             const double s = dx * dx + dy * dy + dz * dz;

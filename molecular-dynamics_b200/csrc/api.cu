@@ -232,6 +232,7 @@ std::vector<SlabItem> slab_items(State& s) {
     for (int** q : keep) v.push_back(item(q, 1, true));
     int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.nbn, &s.slot_cell, &s.chain};
     for (int** q : scratch) v.push_back(item(q, 1, false));
+    v.push_back(item(&s.posb, 1, false));
     v.push_back(item(&s.img_cnt, 2, false));
     v.push_back(item(&s.img_slot, kImgW, false));
     v.push_back(item(&s.dl_buf, 10, false));  // host-mirror transfers: mass, pos[3], vel[3], frc[3]
@@ -241,17 +242,17 @@ std::vector<SlabItem> slab_items(State& s) {
 void free_all(State& s) {
     for (SlabItem& it : slab_items(s)) *it.p = nullptr;  // carved from the slab, freed with it
     dfree(&s.slab);
-    int** ip[] = {&s.cnt, &s.cstart, &s.bcount, &s.scan_part, &s.tile_desc, &s.tile_rows};
+    int** ip[] = {&s.cnt, &s.cstart, &s.bcount, &s.scan_part};
     for (int** q : ip) dfree(q);
     s.img_ok = 0;
     s.ghosts_pushed = 0;
     dfree(&s.bmask);
     dfree(&s.nbl);
-    dfree(&s.tile_stream);
-    s.tile_stream_len = 0;
-    s.tiles_valid = 0;
-    s.tile_desc_blocks = 0;
     dfree(&s.red_part);
+    if (s.ev_counted) {
+        cudaEventDestroy(s.ev_counted);
+        s.ev_counted = nullptr;
+    }
     dfree(&s.thermo_dev);
     dfree(&s.status_dev);
     s.scan_part_cap = 0;
@@ -295,12 +296,14 @@ bool grow_atoms(State& s, int need) {
     return true;
 }
 
+// list capacity in entries per atom, a multiple of four (the list is stored in quads)
+int list_rows(int rows) { return (std::max(rows, 4) + 3) & ~3; }
+
 void grow_lists(State& s, int rows) {
     dfree(&s.nbl);
-    s.nb_cap = rows;
+    s.nb_cap = list_rows(rows);
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
     s.lists_valid = 0;
-    s.tiles_valid = 0;
 }
 
 namespace {
@@ -316,9 +319,9 @@ bool allocate_state(State& s, int N, int nb_cap) {
     const int nblk = border_blocks(std::max(N, 1));
     dalloc(&s.bcount, (size_t)2 * 26 * nblk + 1);
     s.nb_stride = ((std::max(N, 1) + 31) / 32) * 32;
-    s.nb_cap = nb_cap > 0 ? nb_cap : 100;
-    s.tile_cap = 2560;  // tiled-builder halo capacity, grown per grid as halos need
+    s.nb_cap = list_rows(nb_cap > 0 ? nb_cap : 100);
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+    if (!s.ev_counted) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_counted, cudaEventDisableTiming));
     dalloc(&s.thermo_dev, 8);
     dalloc(&s.status_dev, 1);
     if (!s.status_host) TMD_CUDA(cudaMallocHost((void**)&s.status_host, sizeof(DevStatus)));
@@ -736,12 +739,13 @@ void md_distribute_particles(void) {
 void md_assemble_neighborlists(bool half, double cutoff) {
     State& s = g_state;
     if (!require_alive("md_assemble_neighborlists")) return;
-    // pending ghost links stay pending: the list build runs them as extra blocks (nothing
-    // else is pending after md_distribute_particles, which set them last)
-    const bool links = s.pend_links;
-    s.pend_links = false;
+    // pending ghost links stay pending when nothing else is (the list build then runs them as
+    // extra blocks); any other pending work may read them, so then they go first, alone
+    const bool hold = s.pend_links && !s.pend_force.valid && !s.pend_final && !s.pend_ghost && !s.pend_init &&
+                      !s.pend_kick;
+    if (hold) s.pend_links = false;
     flush_all(s);
-    s.pend_links = links;
+    if (hold) s.pend_links = true;
     phase_mark(PH_NEIGH);
     run_build_lists(s, half, cutoff);
 }
@@ -868,7 +872,7 @@ void md_final_integration(double dt) {
     run_final(s, dt);
 }
 
-// core/grid.impala:497-513 (host mirror)
+// core/grid.impala:483-499 (host mirror)
 int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
     State& s = g_state;
     if (!require_alive("md_write_grid_data_to_arrays")) return 0;
@@ -883,7 +887,7 @@ int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* 
     return s.N;
 }
 
-// core/grid.impala:515-532: returns nparticles, as the reference does
+// core/grid.impala:501-518: returns nparticles, as the reference does
 int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
     State& s = g_state;
     if (!require_alive("md_write_grid_ghost_data_to_arrays")) return 0;
@@ -900,7 +904,7 @@ int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vect
     return s.N;
 }
 
-// core/grid.impala:534-560
+// core/grid.impala:520-546
 int md_write_grid_aabb_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
     State& s = g_state;
     const Geometry& g = s.geo;
@@ -1092,27 +1096,6 @@ void md_set_precision(int mode) {
     }
     s.precision = mode;
 }
-void md_set_tile_mode(int enable) {
-    if (g_state.alive) flush_all(g_state);
-    g_state.tile_mode = enable ? 1 : 0;
-    g_state.lists_valid = 0;
-    g_state.tiles_valid = 0;
-}
-void md_tile_info(int* out) {
-    State& s = g_state;
-    if (s.alive) flush_all(s);
-    out[0] = s.tiles_valid;
-    out[1] = s.tile_cap;
-    out[2] = s.tile_halo_max;
-    out[3] = s.nb_cap;
-    out[4] = s.status_host ? s.status_host->tile_overflow : 0;
-    out[5] = s.status_host ? s.status_host->halo_max : 0;
-}
-int md_tiles_active(void) {
-    if (!g_state.alive) return 0;
-    flush_all(g_state);
-    return g_state.tiles_valid;
-}
 void md_set_half_mode(int ghost_pairs) {
     if (g_state.alive) flush_all(g_state);
     g_state.half_ghost = ghost_pairs ? 1 : 0;
@@ -1194,7 +1177,7 @@ int md_get_neighbor_lists(int* sizes, int* lists, int capacity) {
         sizes[r] = n[slot];
         mx = std::max(mx, n[slot]);
         for (int k = 0; k < n[slot] && k < capacity && k < s.nb_cap; ++k)
-            lists[(size_t)r * capacity + k] = ref[l[(size_t)k * s.nb_stride + slot] >> kCodeBits];
+            lists[(size_t)r * capacity + k] = ref[l[(((size_t)(k >> 2) * s.nb_stride + slot) << 2) + (k & 3)] >> kCodeBits];
     }
     return mx;
 }

@@ -2,10 +2,10 @@
 //   * LJ forces over full or half lists, FP64 (bit-identical to the CPU
 //     restatement for full lists) or mixed (FP32 pair arithmetic on rebased
 //     FP32 positions), optionally fused with the final velocity half-kick
-//     (core/compute.impala:79-126, core/runtime.impala:188-201, 186-194)
+//     (core/compute.impala:1-95 and 108-116, core/runtime.impala:188-201)
 //   * DEM spring-dashpot forces (core/runtime.impala:203-247)
 //   * initial integration fused with the periodic ghost refresh
-//     (core/compute.impala:175-184, comm/comm.impala:334-388)
+//     (core/compute.impala:97-106, comm/comm.impala:334-388)
 //   * stand-alone ghost refresh and final integration
 //   * deterministic FP64 reductions of energy, virial and kinetic energy
 //
@@ -58,22 +58,27 @@ __device__ __forceinline__ void put_partial(double* part, int q, double v, doubl
 }
 
 // ---- list prefetch ---------------------------------------------------------------
-// Issues one bulk L2 prefetch per list row the block will read (the block's
-// 256 atoms are one contiguous 1 KiB segment of each row of the atom-fastest
-// list), so the whole list tile is in flight before the neighbour loop.
+// Issues one bulk L2 prefetch per quad row of the list the block will read (the block's
+// atoms are one contiguous segment of 16 bytes per atom in each quad row), so the whole
+// list tile is in flight before the neighbour loop.
 __device__ __forceinline__ void prefetch_list_rows(const uint32_t* nbl, int n, int stride, int nbcap) {
     __shared__ int s_rows;
     if (threadIdx.x == 0) s_rows = 0;
     __syncthreads();
-    if (n > 0) atomicMax(&s_rows, min(n, nbcap));
+    if (n > 0) atomicMax(&s_rows, (min(n, nbcap) + 3) >> 2);
     __syncthreads();
     const int base = blockIdx.x * blockDim.x;
     const int cols = min((int)blockDim.x, stride - base);
     if (cols <= 0) return;
     for (int r = threadIdx.x; r < s_rows; r += blockDim.x) {
-        const uint32_t* p = nbl + (size_t)r * stride + base;
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(cols * 4) : "memory");
+        const uint4* p = reinterpret_cast<const uint4*>(nbl) + (size_t)r * stride + base;
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(cols * 16) : "memory");
     }
+}
+
+// quad b of atom i's list (entries 4b .. 4b + 3)
+__device__ __forceinline__ uint4 list_quad(const uint32_t* nbl, int b, int i, int stride) {
+    return __ldg(reinterpret_cast<const uint4*>(nbl) + (size_t)b * stride + i);
 }
 
 // this block's share of a per-slot array (bytes a multiple of 16), prefetched into L2 by
@@ -101,16 +106,10 @@ __device__ __forceinline__ void add_force32(float4* f, float x, float y, float z
 __device__ __forceinline__ int reaction_slot(int j, int N, const int* groot) { return j < N ? j : groot[j - N]; }
 
 // ---- FP64 LJ ------------------------------------------------------------------
-#ifndef TMD_B64
-#define TMD_B64 4
-#endif
-#ifndef TMD_B32
-#define TMD_B32 4
-#endif
 #ifndef TMD_MINB
 #define TMD_MINB (1024 / TMD_THREADS)  // caps registers at 64 per thread
 #endif
-// v += dt/2 f; x += dt v (core/compute.impala:175-184) in the reference's operand order
+// v += dt/2 f; x += dt v (core/compute.impala:97-106) in the reference's operand order
 __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, double fx, double fy, double fz,
                                                  double dt, double h) {
     v.x = dadd(v.x, dmul(fx, h));
@@ -119,8 +118,8 @@ __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, d
     return make_double4(dadd(x.x, dmul(v.x, dt)), dadd(x.y, dmul(v.y, dt)), dadd(x.z, dmul(v.z, dt)), x.w);
 }
 
-constexpr int kB64 = TMD_B64;  // neighbours loaded per batch (FP64)
-constexpr int kB32 = TMD_B32;  // neighbours loaded per batch (mixed)
+constexpr int kB64 = 4;  // neighbours per batch (FP64): one list quad
+constexpr int kB32 = 4;  // neighbours per batch (mixed): one list quad
 
 // Ghost images written by the force kernel that integrates (maps from k_ghost_links): each
 // local writes the ghosts that are its images, from its new position, and extra threads
@@ -209,24 +208,20 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
     if (i < a.N) {
         const double4 pi = pos[i];
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        const uint32_t* lp = nbl + i;
-        const uint32_t pad = (uint32_t)i << kCodeBits;  // the atom itself, skipped below
-        uint32_t ent[kB64];
-#pragma unroll
-        for (int u = 0; u < kB64; ++u) ent[u] = u < n ? __ldg(lp + (size_t)u * a.stride) : pad;
-        for (int k0 = 0; k0 < n; k0 += kB64) {
+        // quads of four entries; the next quad loads while this one's gathers are in flight
+        // (entries past n are padding, skipped below)
+        const int nq = (n + 3) >> 2;
+        uint4 eq = n > 0 ? list_quad(nbl, 0, i, a.stride) : make_uint4(0u, 0u, 0u, 0u);
+        for (int b = 0; b < nq; ++b) {
+            const int k0 = 4 * b;
+            const uint32_t ent[kB64] = {eq.x, eq.y, eq.z, eq.w};
             int j[kB64];
             double4 pj[kB64];
 #pragma unroll
             for (int u = 0; u < kB64; ++u) j[u] = (int)(ent[u] >> kCodeBits);
 #pragma unroll
             for (int u = 0; u < kB64; ++u) pj[u] = ldg_d4(pos + j[u]);
-            // the next batch's entries load while this batch's gathers are in flight
-#pragma unroll
-            for (int u = 0; u < kB64; ++u) {
-                const int q = k0 + kB64 + u;
-                ent[u] = q < n ? __ldg(lp + (size_t)q * a.stride) : pad;
-            }
+            eq = list_quad(nbl, min(b + 1, nq - 1), i, a.stride);
 #pragma unroll
             for (int u = 0; u < kB64; ++u) {
                 const double dx = dsub(pi.x, pj[u].x), dy = dsub(pi.y, pj[u].y), dz = dsub(pi.z, pj[u].z);
@@ -260,7 +255,7 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
             atomicAdd(&frc[i].z, fz);
         } else {
             frc[i] = make_double4(fx, fy, fz, 0.0);
-            if (FUSE) {  // core/compute.impala:186-194
+            if (FUSE) {  // core/compute.impala:108-116
                 double4 v = vel[i];
                 v.x = dadd(v.x, dmul(fx, a.h));
                 v.y = dadd(v.y, dmul(fy, a.h));
@@ -338,13 +333,12 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
-        const uint32_t* lp = nbl + i;
-        for (int k0 = 0; k0 < n; k0 += kB32) {
-            uint32_t ent[kB32];
+        const int nq = (n + 3) >> 2;
+        for (int b = 0; b < nq; ++b) {
+            const int k0 = 4 * b;
+            const uint4 eq = list_quad(nbl, b, i, a.stride);  // entries past n are padding (skipped)
+            const uint32_t ent[kB32] = {eq.x, eq.y, eq.z, eq.w};
             float4 rj[kB32];
-#pragma unroll
-            for (int u = 0; u < kB32; ++u)
-                ent[u] = (k0 + u < n) ? __ldg(lp + (size_t)(k0 + u) * a.stride) : ((uint32_t)i << kCodeBits) | 21u;
 #pragma unroll
             for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (ent[u] >> kCodeBits));
 #pragma unroll
@@ -450,25 +444,18 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
         int nq = 0, q0 = 0, q1 = 0;  // deferred FP64 pairs
-        const uint32_t* lp = nbl + i;
-        // padding: the atom itself one rebasing cell away on every axis (rsq = 3h^2 with h above
-        // the list cutoff, beyond every window), so it is neither a fast nor a queued pair
-        const uint32_t pad = ((uint32_t)i << kCodeBits) | 42u;
-        uint32_t ent[kB32];
-#pragma unroll
-        for (int u = 0; u < kB32; ++u) ent[u] = u < n ? __ldg(lp + (size_t)u * a.stride) : pad;
-        for (int k0 = 0; k0 < n; k0 += kB32) {
+        // the last quad is padded with the atom itself one rebasing cell away on every axis
+        // (rsq = 3h^2 with h above the list cutoff, beyond every window), so a padding entry
+        // is neither a fast nor a queued pair and the loop needs no count test
+        const int nquad = (n + 3) >> 2;
+        uint4 eq = n > 0 ? list_quad(nbl, 0, i, a.stride) : make_uint4(0u, 0u, 0u, 0u);
+        for (int b = 0; b < nquad; ++b) {
+            const uint32_t cur[kB32] = {eq.x, eq.y, eq.z, eq.w};
             float4 rj[kB32];
 #pragma unroll
-            for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (ent[u] >> kCodeBits));
-            uint32_t cur[kB32];
-#pragma unroll
-            for (int u = 0; u < kB32; ++u) cur[u] = ent[u];
-#pragma unroll
-            for (int u = 0; u < kB32; ++u) {
-                const int q = k0 + kB32 + u;
-                ent[u] = q < n ? __ldg(lp + (size_t)q * a.stride) : pad;
-            }
+            for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (cur[u] >> kCodeBits));
+            // the next quad loads while this one's gathers are in flight
+            eq = list_quad(nbl, min(b + 1, nquad - 1), i, a.stride);
             unsigned slow = 0;
 #pragma unroll
             for (int u = 0; u < kB32; ++u) {
@@ -605,8 +592,10 @@ k_dem_fp64(const double4* __restrict__ pos, const double4* __restrict__ vel, dou
     // penetration test never passes): the loop would only add +0.0
     const int n = a.fixed ? min(nbn[i], a.nbcap) : 0;
     double F[3] = {0.0, 0.0, 0.0};
+    uint4 eq = make_uint4(0u, 0u, 0u, 0u);
     for (int k = 0; k < n; ++k) {
-        const int j = (int)(__ldg(nbl + (size_t)k * a.stride + i) >> kCodeBits);
+        if ((k & 3) == 0) eq = list_quad(nbl, k >> 2, i, a.stride);
+        const int j = (int)((k & 2 ? (k & 1 ? eq.w : eq.z) : (k & 1 ? eq.y : eq.x)) >> kCodeBits);
         const double4 pj = ldg_d4(pos + j);
         const double4 del = make_double4(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z), 0.0);
         const double rsq = len2_strict(del.x, del.y, del.z);
@@ -658,8 +647,10 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
         const double4 vi = vel[i];
         const float vix = (float)vi.x, viy = (float)vi.y, viz = (float)vi.z;
         const int n = min(nbn[i], a.nbcap);
+        uint4 eq = make_uint4(0u, 0u, 0u, 0u);
         for (int k = 0; k < n; ++k) {
-            const uint32_t en = __ldg(nbl + (size_t)k * a.stride + i);
+            if ((k & 3) == 0) eq = list_quad(nbl, k >> 2, i, a.stride);
+            const uint32_t en = k & 2 ? (k & 1 ? eq.w : eq.z) : (k & 1 ? eq.y : eq.x);
             const int j = (int)(en >> kCodeBits);
             const float4 rj = __ldg(pos32 + j);
             const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
@@ -731,7 +722,7 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
 //         edge / corner ghosts lag, exactly like comm/comm.impala:334-388);
 //     2 = exact periodic images: ghost = integrated root + total shift.
 
-// v += h f in the reference's operand order (core/compute.impala:186-194), as k_final does it
+// v += h f in the reference's operand order (core/compute.impala:108-116), as k_final does it
 __device__ __forceinline__ void kick(double4& v, double fx, double fy, double fz, double h) {
     v.x = dadd(v.x, dmul(fx, h));
     v.y = dadd(v.y, dmul(fy, h));
@@ -976,15 +967,23 @@ void check_mixed_cutoff(const State& s, const LjArgs& a) {
         set_error(3, "mixed form: LJ cutoff beyond sqrt(3) cell spacings");
 }
 
+// A list entry's code holds one rebasing-cell step per axis, which needs every listed pair
+// closer than the rebasing spacing (above the cell spacing): a list cutoff beyond it, or a
+// grid too wide for the packed cells, leaves the mixed form's codes invalid.  Latches 3.
+bool mixed_lists_ok(const State& s) {
+    const Geometry& g = s.geo;
+    bool ok = s.lists_cutoff < g.rb_h;
+    for (int d = 0; d < 3; ++d) ok = ok && (g.aabb_hi[d] - g.aabb_lo[d]) / g.rb_h < 1000.0;
+    if (!ok) set_error(3, "mixed form: list cutoff beyond the rebasing spacing or grid too wide");
+    return ok;
+}
+
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
     const int N = s.N;
     if (N == 0) return;
-    if (s.precision == 1 && !p.half && s.tiles_valid && !s.lists_half) {
-        run_force_lj_tiles(s, p, fuse_final, dt);
-        return;
-    }
     LjArgs a = lj_args(s, p, dt);
     if (s.precision == 1 && !p.half) check_mixed_cutoff(s, a);
+    if (s.precision == 1) mixed_lists_ok(s);
     // the list entry's code holds dk + 1 in bits 0-1 (x), 2-3 (y), 4-5 (z)
     a.hx = (float)(-s.geo.rb_h);
     a.hy = (float)(-s.geo.rb_h / 4.0);
@@ -1028,14 +1027,17 @@ void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt) {
 
 bool force_init_fusable(const State& s, const PendingForce& p) {
     // ghost velocities of the contact-fixed DEM model come from k_integrate
-    return !p.dem && !p.half && !s.lists_half && s.dem_fixed == 0 && !(s.precision == 1 && s.tiles_valid);
+    return !p.dem && !p.half && !s.lists_half && s.dem_fixed == 0;
 }
 
 void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double dt_init) {
     const int N = s.N;
     if (N == 0) return;  // no ghosts either
     LjArgs a = lj_args(s, p, dt_final);
-    if (s.precision == 1) check_mixed_cutoff(s, a);
+    if (s.precision == 1) {
+        check_mixed_cutoff(s, a);
+        mixed_lists_ok(s);
+    }
     a.hx = (float)(-s.geo.rb_h);
     a.hy = (float)(-s.geo.rb_h / 4.0);
     a.hz = (float)(-s.geo.rb_h / 16.0);
@@ -1115,6 +1117,7 @@ void run_force_dem(State& s, const PendingForce& p) {
     a.mu = p.mu;
     a.radius = s.dem_radius;
     if (s.precision == 1) {  // the mixed form's integrators read frc32
+        mixed_lists_ok(s);
         DemMixedArgs b;
         const double d2 = 2.0 * (s.dem_fixed ? s.dem_radius : 1.0);
         b.rc2_lo = (float)(a.rc2 * (1.0 - 1e-4));

@@ -13,6 +13,12 @@ constexpr int kCodeBits = 6;
 constexpr uint32_t kCodeMask = (1u << kCodeBits) - 1u;
 constexpr int kMaxSlots = 1 << (32 - kCodeBits);
 
+// Neighbour-list layout: quads of four consecutive entries of one atom, atom-fastest.
+// Entry k of atom i sits at nl_index(k, i, stride); quad b of atom i is uint4 b * stride + i.
+__device__ __forceinline__ size_t nl_index(int k, int i, int stride) {
+    return (((size_t)(k >> 2) * stride + i) << 2) + (k & 3);
+}
+
 // ---- strict FP64 arithmetic (round-to-nearest, never contracted into FMA) --
 // The FP64 form evaluates every expression in the reference's operand order
 // with these, which makes it bit-identical to the CPU restatement.

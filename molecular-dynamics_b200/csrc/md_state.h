@@ -99,12 +99,7 @@ struct DevStatus {
     int nchain;         // ghosts whose two-phase source is a ghost (last distribution)
     int img_over1;      // locals with more than kImg1 direct images
     int img_over2;      // locals with more than kImg2 images in all
-    // zeroed together before a list build (one memset): max_nb .. tile_blocks
-    int max_nb;         // longest neighbour list of the last build
-    int bad_code;       // list pairs whose rebasing offset exceeded one cell
-    int tile_overflow;  // slot blocks the tiled builder could not take (halo or row limits)
-    int halo_max;       // largest staged halo of the last tiled build
-    int tile_blocks;    // row blocks of the last tiled build
+    int max_nb;         // longest neighbour list of the last build (zeroed before each build)
 };
 
 // periodic images a local can push (two-phase: its own first-pass images, one per face
@@ -185,26 +180,20 @@ struct State {
     int* broot_ref = nullptr;    // per ghost: root local reference index
     int* bcode = nullptr;        // per ghost: shift code (reference order)
     // neighbour lists
+    // list layout: quads of four consecutive entries of one atom, atom-fastest (nl_index);
+    // nb_cap is a multiple of four
     int* nbn = nullptr;
     uint32_t* nbl = nullptr;
-    // tiled full lists (k_tile.cu): per warp of a row block, its homes' lists of
-    // halo indices into the block's staged candidates, concatenated home-major
-    uint16_t* tile_stream = nullptr;
-    size_t tile_stream_len = 0;
-    int tile_mode = 0;       // build and use tiled full lists where the grid allows (opt-in)
-    int tiles_valid = 0;     // tile_stream matches the current cells
-    int tile_halo_max = 0;   // largest halo of the current tiled lists (staged atoms)
-    int tile_cap = 2560;     // halo capacity of the tiled builder (grows to fit)
-    int* tile_desc = nullptr;  // per row block: homes, runs and halo ranges (k_tile.cu)
-    int* tile_rows = nullptr;  // per row of cells: blocks, then their exclusive scan
-    int tile_desc_blocks = 0;  // descriptor capacity (blocks)
-    int tile_blocks = 0;       // row blocks of the current tiled lists
+    float4* posb = nullptr;   // per slot: FP32 position relative to the grid origin, w = rbk (list build)
+    double lists_cutoff = 0.0;
     // scan scratch, reductions, status
     int* scan_part = nullptr;  int scan_part_cap = 0;
     double* red_part = nullptr; int red_part_cap = 0;
     double* thermo_dev = nullptr;   // [8]
     DevStatus* status_dev = nullptr;
     DevStatus* status_host = nullptr;  // pinned
+    cudaEvent_t ev_counted = nullptr;  // the ghost count's readback (run_borders)
+    int scan_attr_device = -1;         // device whose k_scan_single shared-memory attribute is set
     double* thermo_host = nullptr;     // pinned [8]
 
     // host mirror in reference order (core/grid.impala ArrayData host buffers)
@@ -270,12 +259,6 @@ void flush_links(State& s);                      // the deferred ghost links of 
 void run_borders(State& s, bool wrap = false);   // ghost generation, reference order (wrap: the periodic wrap first)
 void run_distribute(State& s);                    // binning + reorder
 int run_build_lists(State& s, bool half, double cutoff);  // returns 0 or error
-// tiled full-list build (k_tile.cu): 1 = built, 0 = not applicable (caller builds
-// the plain list), -1 = error
-int run_build_tiles(State& s, double cutoff);
-bool tiles_usable(const State& s);
-bool tile_cap_fits(const State& s, int cap);  // the tiled builder can stage halos of `cap` atoms
-void run_force_lj_tiles(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_dem(State& s, const PendingForce& p);
 // kick_dt >= 0: the previous step's final kick of kick_dt is applied first (held back by

@@ -31,7 +31,9 @@ constexpr int kNoAllocQ = 3;  // energy, virial, pairs inside the cutoff
 // per-block partial sums, quantity-major: [kNoAllocQ][kNoAllocMaxBlocks]
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocQ * kNoAllocMaxBlocks];
 
-// device address of g_noalloc_partials, looked up once per device
+// device address of g_noalloc_partials, looked up once per device; a device reset (or a
+// primary context destroyed and made again) invalidates it, so such a reset needs the library
+// to be loaded again before this entry point is called
 constexpr int kMaxDevices = 64;
 void* g_partials_addr[kMaxDevices] = {nullptr};
 
@@ -104,7 +106,11 @@ using namespace tmd;
 extern "C" int md_lj_forces_noalloc(const double* positions, int n_local, const int* list_sizes,
                                     const int* lists, int stride, int max_neighbors, double cutoff,
                                     double epsilon, double sigma, double* forces, double* sums, void* stream) {
-    if (n_local < 0 || n_local > kNoAllocMaxBlocks * kNoAllocThreads) {
+    if (n_local < 0) {
+        set_error(MD_ERR_ARGUMENT, "md_lj_forces_noalloc: invalid arguments (negative local atom count)");
+        return MD_ERR_ARGUMENT;
+    }
+    if (n_local > kNoAllocMaxBlocks * kNoAllocThreads) {
         char msg[160];
         std::snprintf(msg, sizeof msg, "md_lj_forces_noalloc: %d local atoms exceed the fixed scratch (at most %d)",
                       n_local, kNoAllocMaxBlocks * kNoAllocThreads);

@@ -66,9 +66,6 @@ _EXTENSION_API = {
     "md_set_precision": (None, [_c_int]),
     "md_set_ghost_mode": (None, [_c_int]),
     "md_set_half_mode": (None, [_c_int]),
-    "md_set_tile_mode": (None, [_c_int]),
-    "md_tiles_active": (_c_int, []),
-    "md_tile_info": (None, [_vp]),
     "md_set_dem_model": (None, [_c_int, _c_double]),
     "md_set_thermo": (None, [_c_int]),
     "md_get_thermo": (_c_int, [_vp]),

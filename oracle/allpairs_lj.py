@@ -3,7 +3,7 @@
 Naive O(N^2) forces with minimum-image periodic boundaries and the hard cutoff
 of the reference's LJ closure (core/runtime.impala:188-201; the same force form
 as naive/main.cpp:24-46), velocity-Verlet with unit masses
-(core/compute.impala:175-194), and the trajectory loss of the differentiable
+(core/compute.impala:97-116), and the trajectory loss of the differentiable
 form: mean squared (unwrapped) displacement plus potential energy per atom.
 torch.autograd through this function is the reference the hand-written
 adjoint kernels are checked against.

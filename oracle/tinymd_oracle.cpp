@@ -672,7 +672,7 @@ void md_compute_dem(bool half, double rc, double damping_n, double damping_t, do
     compute_dem(half ? 1 : 0, rc, damping_n, damping_t, stiffness, friction);
 }
 
-// core/compute.impala:175-184
+// core/compute.impala:97-106
 void md_initial_integration(double dt) {
     const int N = g.nparticles;
     const double h = 0.5 * dt;
@@ -687,7 +687,7 @@ void md_initial_integration(double dt) {
     integration_iters = N;
 }
 
-// core/compute.impala:186-194
+// core/compute.impala:108-116
 void md_final_integration(double dt) {
     const int N = g.nparticles;
     const double h = 0.5 * dt;
@@ -700,12 +700,12 @@ void md_final_integration(double dt) {
     integration_iters = N;
 }
 
-// core/compute.impala:196-200
+// core/compute.impala:118-122
 void md_enforce_pbc(void) {
     for (int i = 0; i < g.nparticles; ++i) pbc_correct(P(g.pos, i));
 }
 
-// core/grid.impala:497-513
+// core/grid.impala:483-499
 int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
     for (int i = 0; i < g.nparticles; ++i) {
         m[i] = g.mass[i];
@@ -716,7 +716,7 @@ int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* 
     return g.nparticles;
 }
 
-// core/grid.impala:515-532 (note: returns nparticles, as the reference does)
+// core/grid.impala:501-518 (note: returns nparticles, as the reference does)
 int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
     for (int p = g.nparticles; p < g.nparticles + g.nghost; ++p) {
         int i = p - g.nparticles;
@@ -728,7 +728,7 @@ int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vect
     return g.nparticles;
 }
 
-// core/grid.impala:534-560
+// core/grid.impala:520-546
 int md_write_grid_aabb_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* f) {
     for (int i = 0; i < 2; ++i)
         for (int j = 0; j < 2; ++j)

@@ -6,12 +6,13 @@ also run live on more sizes.
 """
 import ctypes
 import os
+import sys
 
 import numpy as np
 import pytest
 
 import tinymd
-from conftest import GOLDEN
+from conftest import GOLDEN, ROOT
 
 CASES = [("default", (4, 4, 4)), ("default", (5, 7, 6)), ("half", (6, 6, 6)), ("granular_gas", (6, 6, 6)),
          ("body_collision", (3, 3, 3))]
@@ -55,3 +56,15 @@ def test_velocity_stream_is_park_miller(product):
     m, x, v, world, rank = tinymd.setup_particles("default", (4, 4, 4), lib=product)
     # site (0,0,0) has seed 1: its velocity components are draws 6, 12 and 18
     assert tuple(v[0]) == (draws[5], draws[11], draws[17])
+
+
+def test_bench_cpu_lattice_is_the_reference_generator(product, refsetup):
+    """bench.py's CPU arm takes its lattice from oracle/ref_lattice.py (the reference's own
+    initialize.h, no product code): the same particles and boxes as the product's setup."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_lattice
+    for bench, cells in (("default", (8, 8, 8)), ("half", (6, 6, 6))):
+        got = ref_lattice.reference_lattice(cells, bench)
+        want = tinymd.setup_particles(bench, cells, lib=product)
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a, b)

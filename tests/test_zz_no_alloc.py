@@ -67,3 +67,8 @@ def test_noalloc_rejects_too_many_atoms(product):
     assert rc == 3
     assert b"exceed the fixed scratch" in product.md_last_error_string()
     product.md_clear_error()
+    rc = product.md_lj_forces_noalloc(ctypes.c_void_p(16), -1, ctypes.c_void_p(16), ctypes.c_void_p(16), 32, 1, 2.5,
+                                      1.0, 1.0, ctypes.c_void_p(16), ctypes.c_void_p(16), None)
+    assert rc == 3
+    assert b"invalid arguments" in product.md_last_error_string()
+    product.md_clear_error()
