@@ -232,7 +232,6 @@ std::vector<SlabItem> slab_items(State& s) {
     for (int** q : keep) v.push_back(item(q, 1, true));
     int** scratch[] = {&s.bin_cell, &s.bin_rank, &s.tmp_key, &s.tmp_src, &s.nbn, &s.slot_cell, &s.chain};
     for (int** q : scratch) v.push_back(item(q, 1, false));
-    v.push_back(item(&s.posb, 1, false));
     v.push_back(item(&s.img_cnt, 2, false));
     v.push_back(item(&s.img_slot, kImgW, false));
     v.push_back(item(&s.dl_buf, 10, false));  // host-mirror transfers: mass, pos[3], vel[3], frc[3]
@@ -1050,6 +1049,9 @@ void md_report_iterations(void) {
         }
         if (s.lists_valid)
             for (int v : n) total += v;
+        // pairs inside the cutoff of the last force call: its lists and positions are the
+        // current ones (a step's last position update precedes its force)
+        if (s.force_cfg.valid) s.rsq_iters = count_pairs_inside(s, s.force_cfg.rc);
     }
     s.force_iters = total;
     std::printf("ForceIters RsqIters IntegrationIters\n");

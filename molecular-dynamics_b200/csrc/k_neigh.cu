@@ -289,7 +289,7 @@ struct MoveArgs {
     const int* img_o; int* img_n;
     int* slot_of_ref; int* rref; int* rbk;
     const int* bin_cell; int* slot_cell;
-    float4* pos32; float4* posb; int* img_cnt; int* img_slot;
+    float4* pos32; int* img_cnt; int* img_slot;
     int capA, N, mixed;
 };
 
@@ -314,9 +314,6 @@ __device__ __forceinline__ void move_slot(int n, int o, const MoveArgs& m, const
     m.slot_of_ref[r] = n;
     const int k = rebase_cell(p, a);
     m.rbk[n] = k;
-    // the list build's FP32 copy, relative to the grid origin, with the packed rebasing cell
-    m.posb[n] = make_float4((float)(p.x - a.alo[0]), (float)(p.y - a.alo[1]), (float)(p.z - a.alo[2]),
-                            __int_as_float(k));
     if (m.mixed) m.pos32[n] = rebased32(p, k, a.alo, a.rb_h);
 }
 
@@ -384,145 +381,232 @@ __global__ void k_ghost_links(LinkArgs l) {
 }
 
 // ---- neighbour lists ---------------------------------------------------------
-// Thread per home atom (core/neighborlist.impala:18-78).  A home walks the 27 stencil cells
-// of its cell in the reference order -- z, y, x offsets -1..1, flat cell index checked
-// against the grid only -- and within each cell its locals, then its ghosts, in slot order
-// (which is reference order: the binning ranks each cell's members by reference index).
-// Cells are sorted by flat index, so the locals of the three cells of a stencil row are one
-// contiguous slot range; a row is walked as one range when none of its cells holds ghosts.
-// The distance test runs in FP32 on copies of the positions relative to the grid origin
-// (posb, written by the binning), and pairs within `margin` of the cutoff take the
-// reference's FP64 test (rsq <= cutoff^2), so membership is exactly the reference's.
+// rebasing cell k relative to b, 8 bits per axis with bias 128 (|k - b| < 128 per axis
+// for atoms a few cells apart); differences of two such values carry no borrow while
+// every axis differs by at most 1
+__device__ __forceinline__ int rel_cell(int k, int b) {
+    return (wrap_diff(unpack_axis(k, 0), unpack_axis(b, 0)) + 128) |
+           ((wrap_diff(unpack_axis(k, 1), unpack_axis(b, 1)) + 128) << 8) |
+           ((wrap_diff(unpack_axis(k, 2), unpack_axis(b, 2)) + 128) << 16);
+}
+
+// Warp per cell (core/neighborlist.impala:18-78), one home atom per lane (32 at a time).  The
+// 27 stencil cells' candidates (locals then ghosts per cell, stencil order) are staged in shared
+// memory, keeping only those within the list cutoff (with the FP32 margin) of the bounding box
+// of the homes, in order; then every lane walks the kept candidates (one broadcast read each)
+// and appends its own pairs, so each list comes out in stencil order -- the reference's, which
+// fixes the FP64 summation order -- with no cross-lane compaction.  Lanes without a home sit
+// far away and never match.  Pairs near the cutoff take the reference's FP64 test
+// (rsq <= cutoff^2), so membership is exactly the reference's.
 //
-// List layout: quads of four consecutive entries of one atom, atom-fastest -- entry k of
-// atom i at index ((k / 4) * stride + i) * 4 + k % 4 (nl_index) -- so a thread writes four
-// entries with one 16-byte store and a force kernel reads four with one 16-byte load, and the
-// quads of a warp's 32 atoms form one 512-byte line.  An entry is slot << 6 | code, code the
-// neighbour's rebasing cell minus the home's (mixed form).  The last quad of a list is padded
-// with the home itself one rebasing cell away on every axis (code 42), which every force
-// kernel either skips by count or finds beyond its cutoff.
-#ifndef TMD_NL_THREADS
-#define TMD_NL_THREADS 128
+// List layout: quads of four consecutive entries of one atom, atom-fastest (nl_index): a force
+// kernel reads four entries with one 16-byte load, and the quads of a warp's 32 atoms form one
+// 512-byte line.  An entry is slot << 6 | code, code = dk + 1 per axis, dk the neighbour's
+// rebasing cell minus the home's (mixed form).  A list's last quad is padded with the home
+// itself one rebasing cell away on every axis (code 42), which every force kernel skips by
+// count or finds beyond its cutoff.
+#ifndef TMD_NL_WARPS
+#define TMD_NL_WARPS 4
 #endif
-constexpr int kNlThreads = TMD_NL_THREADS;
-constexpr uint32_t kPadCode = 42u;  // dk = +1 on every axis
-constexpr int kBias3 = 0x100401;    // +1 in each 10-bit field of a packed rebasing cell
+#ifndef TMD_NL_TILE
+#define TMD_NL_TILE 128
+#endif
+#ifndef TMD_NL_MINB
+#define TMD_NL_MINB 8  // 64 registers: eight blocks of four warps per SM
+#endif
+#ifndef TMD_NL_UNROLL
+#define TMD_NL_UNROLL 4
+#endif
+constexpr int kNlWarps = TMD_NL_WARPS;    // warps (cells) per block
+constexpr int kNlTile = TMD_NL_TILE;      // kept candidates staged per warp before the homes walk them
+constexpr int kNlUnroll = TMD_NL_UNROLL;  // candidates per step of a home's walk
+constexpr uint32_t kPadCode = 42u;        // dk = +1 on every axis
 
 struct NlArgs {
     double cut2;     // cutoff^2 (FP64, the reference's membership test)
     float lo2, hi2;  // FP32 prefilter: certainly inside below lo2, certainly outside above hi2
     int nbcap, stride, N, ncells, nx, nxy;
-};
-
-// Appends entries to one home's list: four at a time leave as one quad.
-struct ListWriter {
-    uint32_t q0, q1, q2, q3;
-    int cnt;
-    uint4* dst;  // the home's quad column (nbl4 + i); quad b at dst[b * stride]
-    int stride, nquads;
-    __device__ __forceinline__ void push(uint32_t e) {
-        q0 = q1;
-        q1 = q2;
-        q2 = q3;
-        q3 = e;
-        ++cnt;
-        if ((cnt & 3) == 0) {
-            const int b = (cnt >> 2) - 1;
-            if (b < nquads) dst[(size_t)b * stride] = make_uint4(q0, q1, q2, q3);
-        }
-    }
-    __device__ __forceinline__ void finish(uint32_t pad) {
-        const int r = cnt & 3;
-        if (r == 0) return;
-        const int b = cnt >> 2;
-        if (b >= nquads) return;
-        uint4 v = make_uint4(pad, pad, pad, pad);
-        if (r == 1) v.x = q3;
-        if (r == 2) v.x = q2, v.y = q3;
-        if (r == 3) v.x = q1, v.y = q2, v.z = q3;
-        dst[(size_t)b * stride] = v;
-    }
+    double alo[3], spacing;
 };
 
 template <int HM>
-__global__ void __launch_bounds__(kNlThreads)
-k_build_list(const float4* __restrict__ posb, const double4* __restrict__ pos, const int* __restrict__ key,
-             const int* __restrict__ slot_cell, const int* __restrict__ cstart, int* __restrict__ nbn,
-             uint4* __restrict__ nbl4, DevStatus* st, NlArgs a, int home_blocks, LinkArgs la) {
-    if (blockIdx.x >= home_blocks) {  // blocks past the homes link the ghosts (k_ghost_links' work)
-        const int h = (blockIdx.x - home_blocks) * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(kNlWarps * 32, TMD_NL_MINB)
+k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
+             const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl, DevStatus* st,
+             NlArgs a, int cell_blocks, LinkArgs la) {
+    __shared__ float4 s_cpos[kNlWarps][kNlTile];  // kept candidate position (cell-centre relative), w = slot << 6
+    __shared__ int s_crel[kNlWarps][kNlTile];     // its rebasing cell relative to the first home's
+    __shared__ int s_cref[kNlWarps][HM ? kNlTile : 1];
+    __shared__ int s_rstart[kNlWarps][54];
+    __shared__ int s_rpre[kNlWarps][55];
+
+    if (blockIdx.x >= cell_blocks) {  // blocks past the cells link the ghosts (k_ghost_links' work)
+        const int h = (blockIdx.x - cell_blocks) * blockDim.x + threadIdx.x;
         if (h < la.G) ghost_link(h, la);
         return;
     }
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int cnt = 0;
-    if (i < a.N) {
-        const int c = slot_cell[i];
-        if (c < a.ncells) {  // locals outside the grid (bucket ncells) get empty lists
-            const float4 hp = __ldg(posb + i);
-            const uint32_t kib = (uint32_t)__float_as_int(hp.w) - (uint32_t)kBias3;
-            const int ikey = HM ? __ldg(key + i) : 0;
-            const int* gcs = cstart + a.ncells + 1;  // ghost CSR
-            ListWriter w;
-            w.q0 = w.q1 = w.q2 = w.q3 = 0u;
-            w.cnt = 0;
-            w.dst = nbl4 + i;
-            w.stride = a.stride;
-            w.nquads = a.nbcap >> 2;
-            // candidates [j0, j1) in slot order; SELF: the range holds the home itself, which is
-            // skipped (one test per candidate there rather than two loops of unequal lengths)
-            auto walk = [&](int j0, int j1, bool self) {
-#pragma unroll 4
-                for (int j = j0; j < j1; ++j) {
-                    const float4 q = __ldg(posb + j);
-                    const float dx = hp.x - q.x, dy = hp.y - q.y, dz = hp.z - q.z;
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    bool in = r2 < a.lo2;
-                    if (!in && r2 <= a.hi2) {
-                        // near the cutoff: the reference's exact FP64 test
-                        const double4 pi = pos[i], pj = pos[j];
-                        in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
-                    }
-                    if (self) in = in && j != i;
-                    // core/neighborlist.impala:34: half lists keep j < i by reference index (HM 1);
-                    // HM 2 compares a ghost by its root, so a boundary pair is kept once
-                    if (HM) in = in && __ldg(key + j) < ikey;
-                    if (in) {
-                        // per-axis (dk + 1) in the 10-bit fields, gathered into bits 0-5
-                        const uint32_t d = (uint32_t)__float_as_int(q.w) - kib;
-                        w.push(((uint32_t)j << kCodeBits) | ((d + (d >> 8) + (d >> 16)) & kCodeMask));
-                    }
-                }
-            };
-            // the 9 stencil rows' cell starts are requested together (L1 prefetch), so each row's
-            // lookups below wait for one cache hit rather than a miss
-#pragma unroll
-            for (int r = 0; r < 9; ++r) {
-                const int rc = min(max(c + (r / 3 - 1) * a.nxy + (r % 3 - 1) * a.nx - 1, 0), a.ncells - 1);
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(cstart + rc));
-                asm volatile("prefetch.global.L1 [%0];" ::"l"(gcs + rc));
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int c = blockIdx.x * kNlWarps + wid;
+    if (c >= a.ncells) return;
+    const int h0 = cstart[c], h1 = cstart[c + 1];
+    if (h0 == h1) return;
+    const unsigned lt = lanemask_lt();
+
+    // 27 stencil cells in the reference order (z, y, x offsets -1..1), each contributing
+    // its locals then its ghosts (54 ranges); lane l owns ranges 2l and 2l + 1
+    {
+        int start = 0, len = 0, gs = 0, gl = 0;
+        if (lane < 27) {
+            const int oz = lane / 9 - 1, oy = (lane / 3) % 3 - 1, ox = lane % 3 - 1;
+            const int nb = c + oz * a.nxy + oy * a.nx + ox;
+            if (nb >= 0 && nb < a.ncells) {
+                start = cstart[nb];
+                len = cstart[nb + 1] - start;
+                gs = cstart[a.ncells + 1 + nb];
+                gl = cstart[a.ncells + 2 + nb] - gs;
             }
-#pragma unroll 1
-            for (int r = 0; r < 9; ++r) {
-                const int rc = c + (r / 3 - 1) * a.nxy + (r % 3 - 1) * a.nx;
-                const int lo = max(rc - 1, 0), hi = min(rc + 1, a.ncells - 1);
-                if (lo > hi) continue;
-                if (__ldg(gcs + lo) == __ldg(gcs + hi + 1)) {  // no ghosts in the row's cells: one range
-                    walk(__ldg(cstart + lo), __ldg(cstart + hi + 1), lo <= c && c <= hi);
-                } else {
-                    for (int k = lo; k <= hi; ++k) {
-                        walk(__ldg(cstart + k), __ldg(cstart + k + 1), k == c);
-                        walk(__ldg(gcs + k), __ldg(gcs + k + 1), false);
-                    }
-                }
-            }
-            w.finish(((uint32_t)i << kCodeBits) | kPadCode);
-            cnt = w.cnt;
         }
-        nbn[i] = cnt;
+        int incl = len + gl;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane < 27) {
+            const int ex = incl - len - gl;
+            s_rstart[wid][2 * lane] = start;
+            s_rstart[wid][2 * lane + 1] = gs;
+            s_rpre[wid][2 * lane] = ex;
+            s_rpre[wid][2 * lane + 1] = ex + len;
+        }
+        if (lane == 26) s_rpre[wid][54] = incl;
     }
-    const int mx = warp_max(cnt);
-    if ((threadIdx.x & 31) == 0 && mx > 0) atomicMax(&st->max_nb, mx);
+    __syncwarp();
+    const int M = s_rpre[wid][54];
+
+    const int cz = c / a.nxy, cy = (c / a.nx) % (a.nxy / a.nx), cx = c % a.nx;
+    const double ctr[3] = {a.alo[0] + ((double)cx + 0.5) * a.spacing, a.alo[1] + ((double)cy + 0.5) * a.spacing,
+                           a.alo[2] + ((double)cz + 0.5) * a.spacing};
+    const int rb0 = __ldg(rbk + h0);  // rebasing cells are staged relative to the first home's
+    int maxcnt = 0;
+
+    for (int hb = h0; hb < h1; hb += 32) {
+        const int hn = min(32, h1 - hb);
+        const bool home = lane < hn;
+        const int i = hb + (home ? lane : 0);
+        const uint32_t i6 = (uint32_t)i << kCodeBits;
+        float hx = 1e18f, hy = 1e18f, hz = 1e18f;  // no home: never within the cutoff
+        int irel = 0, iref = 0;
+        if (home) {
+            const double4 p = pos[i];
+            hx = (float)(p.x - ctr[0]);
+            hy = (float)(p.y - ctr[1]);
+            hz = (float)(p.z - ctr[2]);
+            irel = rel_cell(rbk[i], rb0);
+            if (HM) iref = ref[i];
+        }
+        // bounding box of the homes, widened by the list cutoff (with the FP32 margin)
+        float lo[3] = {home ? hx : INFINITY, home ? hy : INFINITY, home ? hz : INFINITY};
+        float hi[3] = {home ? hx : -INFINITY, home ? hy : -INFINITY, home ? hz : -INFINITY};
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                lo[d] = fminf(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
+                hi[d] = fmaxf(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
+            }
+        int cnt = 0;
+        int t0 = 0;  // next candidate to stage (M > 0: the home cell is in the stencil)
+        do {
+            int nk = 0;  // kept candidates staged (warp-uniform)
+            // stage: keep candidates in order until the next chunk might not fit
+            while (t0 < M && nk + 32 <= kNlTile) {
+                const int m = t0 + lane;
+                bool keep = false;
+                float4 cp;
+                int crel = 0, cref = 0;
+                if (m < M) {
+                    int lo_r = 0, hi_r = 53;  // the range of candidate m: the last one starting at or before m
+                    while (lo_r < hi_r) {
+                        const int mid = (lo_r + hi_r + 1) >> 1;
+                        if (s_rpre[wid][mid] <= m) lo_r = mid;
+                        else hi_r = mid - 1;
+                    }
+                    const int slot = s_rstart[wid][lo_r] + (m - s_rpre[wid][lo_r]);
+                    // the candidate's position, rebasing cell and key load together (one latency)
+                    const double4 p = pos[slot];
+                    const int kb = __ldg(rbk + slot);
+                    if (HM) cref = __ldg(ref + slot);  // root reference index (ref for locals)
+                    cp = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]), (float)(p.z - ctr[2]),
+                                     __uint_as_float((uint32_t)slot << kCodeBits));
+                    const float ex = fmaxf(fmaxf(lo[0] - cp.x, cp.x - hi[0]), 0.f);
+                    const float ey = fmaxf(fmaxf(lo[1] - cp.y, cp.y - hi[1]), 0.f);
+                    const float ez = fmaxf(fmaxf(lo[2] - cp.z, cp.z - hi[2]), 0.f);
+                    keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= a.hi2;
+                    crel = rel_cell(kb, rb0);
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, keep);
+                if (keep) {
+                    const int at = nk + __popc(bal & lt);
+                    s_cpos[wid][at] = cp;
+                    s_crel[wid][at] = crel;
+                    if (HM) s_cref[wid][at] = cref;
+                }
+                nk += __popc(bal);
+                t0 += 32;
+            }
+            __syncwarp();
+            // every home walks the kept candidates in order
+#pragma unroll kNlUnroll
+            for (int k = 0; k < nk; ++k) {
+                const float4 cp = s_cpos[wid][k];
+                const float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const uint32_t s6 = __float_as_uint(cp.w);  // slot << 6
+                bool in = r2 < a.lo2;
+                if (!in && r2 <= a.hi2) {
+                    // near the cutoff: the reference's exact FP64 test
+                    const double4 pi = pos[i], pj = pos[s6 >> kCodeBits];
+                    in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
+                }
+                // core/neighborlist.impala:34: half lists keep i > j (reference index); HM == 2
+                // compares ghosts by their root so pairs across the periodic boundary are kept once
+                const bool take = in && s6 != i6 && (!HM || s_cref[wid][HM ? k : 0] < iref);
+                if (HM) {
+                    // half lists: the append without a branch (measured faster there, while
+                    // the full-list walk is faster with the branch)
+                    const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
+                    const uint32_t code = (d + (d >> 6) + (d >> 12)) & kCodeMask;
+                    if (take && cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 | code;
+                    cnt += take ? 1 : 0;
+                } else if (take) {
+                    // dk + 1 per axis in bytes 0-2, packed as x | y << 2 | z << 4 (the three
+                    // shifted copies land in disjoint bits 0-5 without carries); the list cutoff
+                    // below the rebasing spacing keeps every |dk| <= 1 (checked on the host)
+                    const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
+                    const uint32_t code = (d + (d >> 6) + (d >> 12)) & kCodeMask;
+                    if (cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 | code;
+                    ++cnt;
+                }
+            }
+            __syncwarp();
+        } while (t0 < M);
+        if (home) {
+            nbn[i] = cnt;
+            // the last quad's padding
+            const uint32_t pad = i6 | kPadCode;
+            for (int q = cnt; (q & 3) != 0 && q < a.nbcap; ++q) nbl[nl_index(q, i, a.stride)] = pad;
+            maxcnt = max(maxcnt, cnt);
+        }
+    }
+    maxcnt = warp_max(maxcnt);
+    if (lane == 0) atomicMax(&st->max_nb, maxcnt);
+}
+
+// Locals outside the grid (bucket ncells) get empty lists.
+__global__ void k_clear_lists(int* __restrict__ nbn, int a, int b) {
+    int i = a + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < b) nbn[i] = 0;
 }
 
 // ---- exclusive scan ------------------------------------------------------------
@@ -757,7 +841,7 @@ void run_distribute(State& s) {
     m.img_o = s.img.b[s.ac]; m.img_n = s.img.b[na];
     m.slot_of_ref = s.slot_of_ref; m.rref = s.rref; m.rbk = s.rbk;
     m.bin_cell = s.bin_cell; m.slot_cell = s.slot_cell;
-    m.pos32 = s.pos32.b[np]; m.posb = s.posb; m.img_cnt = s.img_cnt; m.img_slot = s.img_slot;
+    m.pos32 = s.pos32.b[np]; m.img_cnt = s.img_cnt; m.img_slot = s.img_slot;
     m.capA = s.capA; m.N = N; m.mixed = s.precision;
     k_rank_move<<<nblocks((long long)nseg * 32, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, nseg,
                                                                            a.ncells, m, a, s.status_dev);
@@ -818,11 +902,7 @@ int run_build_lists(State& s, bool half, double cutoff) {
     if (half && s.half_ghost) flush_links(s);
     NlArgs a;
     a.cut2 = cutoff * cutoff;
-    // FP32 positions relative to the grid origin carry at most extent * 2^-24 each; a pair's
-    // FP32 rsq is then within 4 sqrt(3) cutoff * that of the FP64 value, far inside the margin
-    double extent = 0.0;
-    for (int d = 0; d < 3; ++d) extent = std::max(extent, g.aabb_hi[d] - g.aabb_lo[d] + 2.0 * cutoff);
-    const double margin = std::max(1e-3 * a.cut2 + 1e-6, 16.0 * cutoff * extent * std::ldexp(1.0, -24));
+    const double margin = 1e-3 * a.cut2 + 1e-6;
     a.lo2 = (float)(a.cut2 - margin);
     a.hi2 = (float)(a.cut2 + margin);
     a.N = s.N;
@@ -830,7 +910,9 @@ int run_build_lists(State& s, bool half, double cutoff) {
     a.nx = g.nx;
     a.nxy = g.nx * g.ny;
     a.stride = s.nb_stride;
-    const int hb = nblocks(s.N, kNlThreads);
+    for (int d = 0; d < 3; ++d) a.alo[d] = g.aabb_lo[d];
+    a.spacing = g.spacing;
+    const int nb = nblocks(g.ncells, kNlWarps);
     for (int attempt = 0; attempt < 8; ++attempt) {
         a.nbcap = s.nb_cap;
         if (attempt > 0 || !s.build_zeroed)  // else zeroed by the binning's reorder kernel
@@ -839,24 +921,30 @@ int run_build_lists(State& s, bool half, double cutoff) {
         prof_begin(K_NLIST);
         // the pending ghost links ride along as extra blocks (once: they count with atomics)
         const LinkArgs la = link_args(s);
-        const int lb = s.pend_links ? nblocks(s.G, kNlThreads) : 0;
+        const int lb = s.pend_links ? nblocks(s.G, kNlWarps * 32) : 0;
         s.pend_links = false;
-        uint4* nbl4 = reinterpret_cast<uint4*>(s.nbl);
         if (half && s.half_ghost)
-            k_build_list<2><<<hb + lb, kNlThreads, 0, s.stream>>>(s.posb, s.pos.b[s.pc], s.rref, s.slot_cell,
-                                                                 s.cstart, s.nbn, nbl4, s.status_dev, a, hb, la);
+            k_build_list<2><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart, s.nbn,
+                                                                     s.nbl, s.status_dev, a, nb, la);
         else if (half)
-            k_build_list<1><<<hb + lb, kNlThreads, 0, s.stream>>>(s.posb, s.pos.b[s.pc], s.ref.b[s.ac], s.slot_cell,
-                                                                 s.cstart, s.nbn, nbl4, s.status_dev, a, hb, la);
+            k_build_list<1><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                     s.nbn, s.nbl, s.status_dev, a, nb, la);
         else
-            k_build_list<0><<<hb + lb, kNlThreads, 0, s.stream>>>(s.posb, s.pos.b[s.pc], nullptr, s.slot_cell,
-                                                                 s.cstart, s.nbn, nbl4, s.status_dev, a, hb, la);
+            k_build_list<0><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
+                                                                     s.nbn, s.nbl, s.status_dev, a, nb, la);
         launched(K_NLIST);
         prof_end(K_NLIST);
         TMD_CUDA(cudaMemcpyAsync(s.status_host, s.status_dev, sizeof(DevStatus), cudaMemcpyDeviceToHost, s.stream));
         TMD_CUDA(cudaStreamSynchronize(s.stream));
-        if (s.status_host->out_local > 0)
+        if (s.status_host->out_local > 0) {
+            int first_out = 0;
+            // locals outside the grid sit at [cstart[ncells], N): empty lists
+            TMD_CUDA(cudaMemcpyAsync(&first_out, s.cstart + g.ncells, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+            TMD_CUDA(cudaStreamSynchronize(s.stream));
+            k_clear_lists<<<nblocks(s.N - first_out, 256), 256, 0, s.stream>>>(s.nbn, first_out, s.N);
+            launched(K_NLIST);
             set_error(5, "locals outside the cell grid at binning (they have no neighbours)");
+        }
         s.nchain = s.status_host->nchain;
         s.img_ok = (s.status_host->img_over1 == 0 ? 1 : 0) | (s.status_host->img_over2 == 0 ? 2 : 0);
         const int mx = s.status_host->max_nb;

@@ -120,6 +120,7 @@ __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, d
 
 constexpr int kB64 = 4;  // neighbours per batch (FP64): one list quad
 constexpr int kB32 = 4;  // neighbours per batch (mixed): one list quad
+constexpr int kQ = 8;    // FP64-path neighbours a mixed thread queues before working them off
 
 // Ghost images written by the force kernel that integrates (maps from k_ghost_links): each
 // local writes the ghosts that are its images, from its new position, and extra threads
@@ -282,6 +283,16 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
 }
 
 // ---- mixed LJ -----------------------------------------------------------------
+// 1/x for the mixed form's FP64 pairs: the hardware's approximate FP64 reciprocal refined by
+// two Newton-Raphson steps (y <- y + y (1 - x y), quadratic convergence), relative error far
+// below the 1e-7 the mixed form's FP64 pairs need, without a full IEEE division
+__device__ __forceinline__ double recip64(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    y = fma(y, fma(-x, y, 1.0), y);
+    return fma(y, fma(-x, y, 1.0), y);
+}
+
 // FP64 evaluation of one list pair (the mixed form's fallback for close pairs
 // and pairs at the cutoff): accumulates the force on i into c and the thermo sums
 template <bool THERMO>
@@ -291,7 +302,7 @@ __device__ __forceinline__ void fp64_lj(const double4& pi, int j, const double4*
     const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
     const double r2 = len2_strict(ex, ey, ez);
     if (r2 < a.rc2) {
-        const double sr2 = 1.0 / r2;
+        const double sr2 = recip64(r2);
         const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
         const double f = 48.0 * sr6 * (sr6 - 0.5) * sr2 * a.eps;
         cx += ex * f;
@@ -376,7 +387,7 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
                     const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
                     const double r2 = len2_strict(ex, ey, ez);
                     if (r2 < a.rc2) {
-                        const double sr2 = 1.0 / r2;
+                        const double sr2 = recip64(r2);
                         const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
                         const double f = 48.0 * sr6 * (sr6 - 0.5) * sr2 * a.eps;
                         cx += ex * f;
@@ -429,6 +440,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
               float4* __restrict__ pos32_n = nullptr, const int* __restrict__ rbk = nullptr,
               PushArgs pa = PushArgs()) {
     __shared__ double scratch[kThreads / 32];
+    __shared__ int s_q[kQ][kThreads];  // each thread's queue of FP64-path neighbours
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_list_rows(nbl, n, a.stride, a.nbcap);
@@ -443,7 +455,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
-        int nq = 0, q0 = 0, q1 = 0;  // deferred FP64 pairs
+        int nq = 0;  // deferred FP64 pairs, in s_q[0..nq)[threadIdx.x]
         // the last quad is padded with the atom itself one rebasing cell away on every axis
         // (rsq = 3h^2 with h above the list cutoff, beyond every window), so a padding entry
         // is neither a fast nor a queued pair and the loop needs no count test
@@ -483,24 +495,24 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
                     ncnt += fast ? 1 : 0;
                 }
             }
-            if (slow) {
-#pragma unroll
-                for (int u = 0; u < kB32; ++u) {
-                    if (!((slow >> u) & 1u)) continue;
-                    const int j = (int)(cur[u] >> kCodeBits);
-                    if (nq == 2) {
-                        fp64_lj_i<THERMO>(pos, i, q0, a, cx, cy, cz, e, w, ncnt);
-                        fp64_lj_i<THERMO>(pos, i, q1, a, cx, cy, cz, e, w, ncnt);
-                        nq = 0;
-                    }
-                    if (nq == 0) q0 = j;
-                    else q1 = j;
-                    ++nq;
+            while (slow) {  // queued in list order; a full queue is worked off first (rare)
+                const int u = __ffs(slow) - 1;
+                slow &= slow - 1u;
+                const uint32_t en = u == 0 ? cur[0] : (u == 1 ? cur[1] : (u == 2 ? cur[2] : cur[3]));
+                if (nq == kQ) {
+                    const double4 pi = ldg_d4(pos + i);
+                    for (int q = 0; q < kQ; ++q) fp64_lj<THERMO>(pi, s_q[q][threadIdx.x], pos, a, cx, cy, cz, e, w, ncnt);
+                    nq = 0;
                 }
+                s_q[nq++][threadIdx.x] = (int)(en >> kCodeBits);
             }
         }
-        if (nq > 0) fp64_lj_i<THERMO>(pos, i, q0, a, cx, cy, cz, e, w, ncnt);
-        if (nq > 1) fp64_lj_i<THERMO>(pos, i, q1, a, cx, cy, cz, e, w, ncnt);
+        // the FP64 pairs of the whole list, worked off together: the warp's lanes run them side
+        // by side instead of one lane at a time inside the loop
+        if (nq > 0) {
+            const double4 pi = ldg_d4(pos + i);
+            for (int q = 0; q < nq; ++q) fp64_lj<THERMO>(pi, s_q[q][threadIdx.x], pos, a, cx, cy, cz, e, w, ncnt);
+        }
         const double Fx = (double)fx + cx, Fy = (double)fy + cy, Fz = (double)fz + cz;
         const float4 F = make_float4((float)Fx, (float)Fy, (float)Fz, 0.f);
         frc32[i] = F;
@@ -875,6 +887,26 @@ k_final(double4* __restrict__ vel, const double4* __restrict__ frc, const float4
         if (THERMO) ke = v.x * v.x + v.y * v.y + v.z * v.z;
     }
     if (THERMO) put_partial(part, 3, ke, scratch);
+}
+
+// List pairs inside the force cutoff (rsq < rc^2 in the reference's FP64 evaluation order):
+// the reference's rsq_iters of the last force call (core/runtime.impala:188-201, 203-247),
+// counted on demand at report time from the lists and positions that call used.
+__global__ void k_count_inside(const double4* __restrict__ pos, const int* __restrict__ nbn,
+                               const uint32_t* __restrict__ nbl, int N, int stride, int nbcap, double rc2,
+                               unsigned long long* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned c = 0;
+    if (i < N) {
+        const double4 pi = pos[i];
+        const int n = min(nbn[i], nbcap);
+        for (int k = 0; k < n; ++k) {
+            const double4 pj = ldg_d4(pos + (int)(nbl[nl_index(k, i, stride)] >> kCodeBits));
+            c += len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) < rc2 ? 1u : 0u;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, (unsigned long long)c);
 }
 
 __global__ void k_refresh_pos32(const double4* __restrict__ pos, float4* __restrict__ pos32,
@@ -1254,6 +1286,19 @@ void run_refresh_pos32(State& s) {
     StepArgs a = step_args(s, 0.0);
     k_refresh_pos32<<<nblocks(NA, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.pos32.b[s.pc], s.rbk, NA, a);
     launched(K_MISC);
+}
+
+long long count_pairs_inside(State& s, double rc) {
+    if (s.N == 0 || !s.lists_valid) return 0;
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(s.thermo_dev + 6);  // spare words
+    TMD_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s.stream));
+    k_count_inside<<<nblocks(s.N, kThreads), kThreads, 0, s.stream>>>(s.pos.b[s.pc], s.nbn, s.nbl, s.N, s.nb_stride,
+                                                                      s.nb_cap, rc * rc, d);
+    launched(K_MISC);
+    unsigned long long h = 0;
+    TMD_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    return (long long)h;
 }
 
 }  // namespace tmd

@@ -45,12 +45,13 @@ inline LjArgs lj_args(const State& s, const PendingForce& p, double dt) {
     const double margin = 2e-5 * a.rc2 + 1e-7;
     a.rc2_lo = (float)(a.rc2 - margin);
     a.rc2_hi = (float)(a.rc2 + margin);
-    // pairs closer than 1.05 sigma take the FP64 path: the force's steep r^-13 branch magnifies
+    // pairs closer than 1.04 sigma take the FP64 path: the force's steep r^-13 branch magnifies
     // the FP32 rounding of del there.  On the 131k-atom LJ liquid (emulated FP32 arithmetic
     // against FP64), max |dF| / rms(F) after 25 / 220 / 1000 steps is 1.30e-5 / 7.2e-6 / 8.0e-6
-    // with a threshold of sigma (~0.1-0.3 FP64 pairs per atom) and 5.7e-6 / 3.9e-6 / 3.8e-6 with
-    // 1.05 sigma (~1.2-1.4 FP64 pairs per atom)
-    a.close2 = (float)((1.05 * p.sigma) * (1.05 * p.sigma));
+    // with a threshold of sigma (~0.1-0.3 FP64 pairs per atom), 9.6e-6 after 25 steps with
+    // 1.02 sigma, 4.5e-6 / 4.7e-6 after 220 / 1000 steps with 1.04 sigma (~1.0 FP64 pair per
+    // atom) and 5.7e-6 / 3.9e-6 / 3.8e-6 with 1.05 sigma (~1.2-1.4 FP64 pairs per atom)
+    a.close2 = (float)((1.04 * p.sigma) * (1.04 * p.sigma));
     a.sig6f = (float)a.sigma6;
     a.eps48f = (float)(48.0 * p.eps);
     a.eps4f = (float)(4.0 * p.eps);

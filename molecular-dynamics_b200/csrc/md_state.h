@@ -184,7 +184,6 @@ struct State {
     // nb_cap is a multiple of four
     int* nbn = nullptr;
     uint32_t* nbl = nullptr;
-    float4* posb = nullptr;   // per slot: FP32 position relative to the grid origin, w = rbk (list build)
     double lists_cutoff = 0.0;
     // scan scratch, reductions, status
     int* scan_part = nullptr;  int scan_part_cap = 0;
@@ -267,6 +266,9 @@ void run_integrate(State& s, double dt, bool fuse_ghosts, double kick_dt = -1.0)
 void run_ghost_sync(State& s);
 void run_final(State& s, double dt);
 void run_refresh_pos32(State& s);
+// list pairs inside the cutoff rc (FP64), the reference's rsq_iters of a force call on the
+// current lists and positions
+long long count_pairs_inside(State& s, double rc);
 // the LJ force (full list) with the final kick of dt_final and the next step's initial
 // integration of dt_init fused into its epilogue (plain-list kernels); writes the locals of
 // the other position buffer, which becomes current (ghosts: run_ghost_refresh)
