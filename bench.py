@@ -337,6 +337,46 @@ def measure(lib, tm, parts, precision, steps, warmup, flush, half=False, force_f
     return len(parts[0]) * steps / (ms * 1e-3), ms / steps, fms
 
 
+def kernel_table(lib, tm, parts, peak, steps=60):
+    """Per kernel class of the mixed 131k workload: mean launch time from CUDA events around every
+    launch (a separate, untimed run: events drain the stream) and the SURVEY 8(d) algorithmic bytes
+    per launch, as GB/s and a fraction of the measured HBM copy bandwidth."""
+    lib.md_set_precision(1)
+    sim = tm.Simulation(lib, *parts, temp=1.44)
+    sim.run(DT, 20)
+    n, g = sim.counts()
+    sizes = np.zeros(n, dtype=np.int32)
+    lists = np.zeros((n, 1), dtype=np.int32)
+    lib.md_get_neighbor_lists(tm.ptr(sizes), tm.ptr(lists), 1)
+    nb = float(sizes.mean())
+    lib.md_profile_enable(0xffff)
+    lib.md_profile_sample(1)
+    lib.md_profile_reset()
+    sim.run(DT, steps)
+    # bytes per launch: force (4 + 16n + 24 per atom, plus the fused integration 5 x 24 per atom and
+    # 55 per ghost), list build (27 x 24 staged + 4n per atom), binning (~128 per slot reordered),
+    # borders (~80 per local scanned, ~200 per ghost written)
+    model = {"force_lj": n * (4 + 16 * nb + 24 + 120) + g * 55, "neighbor_list": n * (27 * 24 + 4 * nb),
+             "binning": (n + g) * 128, "borders": n * 80 + g * 200}
+    out = {}
+    for k in range(lib.md_profile_count()):
+        name = lib.md_profile_name(k).decode()
+        if name not in model:
+            continue
+        nl, t = ctypes.c_longlong(), ctypes.c_double()
+        lib.md_profile_get(k, ctypes.byref(nl), ctypes.byref(t))
+        if nl.value == 0:
+            continue
+        us = t.value * 1e3 / nl.value
+        gbs = model[name] / (us * 1e-6) / 1e9
+        out[name] = {"launches": nl.value, "launch_us": us, "bytes_per_launch": model[name], "GB/s": gbs,
+                     "frac_of_hbm": gbs / peak}
+    lib.md_profile_enable(0)
+    sim.close()
+    lib.md_set_precision(0)
+    return out
+
+
 def workloads(lib, tm, flush, peak):
     """The other measured configurations (atom-steps/s in both forms)."""
     out = {}
@@ -360,7 +400,11 @@ def workloads(lib, tm, flush, peak):
     row["roofline_mixed_force"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                    "frac": achieved / peak, "launch_ms": launch_ms, "bytes_per_atom": b32,
                                    "force_bytes_per_atom": fb, "integrate_ghost_bytes_per_atom": sb,
-                                   "mean_list_length": mean_nb}
+                                   "mean_list_length": mean_nb,
+                                   # ncu at this size: 280 MB of DRAM traffic per launch in 112 us (2.5 TB/s,
+                                   # 0.38 of the measured peak); the neighbour gathers are served by L2
+                                   "traffic": 280.2e6, "traffic_source": "profiles/lj_mixed_full_524k_dram.md",
+                                   "limiter": "instruction issue and latency (78 M warp instructions per launch)"}
     out["lj_half_fcc_64x64x64_524288_atoms_full_list"] = row
     # DEM at 48^3: the FCC diagonal split and the reference's granular gas, with the
     # reference closure (zero force) and the contact-fixed model (R = 0.6)
@@ -479,31 +523,38 @@ def run_ours(args):
         drift["fp64"]["max_abs_drift_per_atom"], 1e-300)
     adj = adjoint_times(lib, tm)
     more = workloads(lib, tm, flush, peaks()[0])
+    ktable = kernel_table(lib, tm, parts, peaks()[0])
 
     # ---- end to end through the C ABI with host buffers ---------------------------
-    lib.md_set_precision(1)
     m, x, v, world_box, rank_box = parts
-    e2e_runs = []
-    for rep in range(3):  # best of three: the host clock also sees the box's other load
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        s = tm.Simulation(lib, m, x, v, world_box, rank_box, temp=1.44)
-        lib.md_synchronize()
-        ta = time.perf_counter()
-        s.run(DT, K)
-        lib.md_synchronize()
-        tb = time.perf_counter()
-        mm, xx, vv, ff = s.arrays()
-        t1 = time.perf_counter()
-        nghost = s.counts()[1]
-        s.close()
-        # (total, set-up: grid, device allocation, upload, first lists and force; steps; copy back)
-        e2e_runs.append((t1 - t0, ta - t0, tb - ta, t1 - tb))
-    best = min(e2e_runs)
+
+    def e2e_best(precision):
+        """Best of three host-clock runs (the host clock also sees the box's other load):
+        (total, set-up: grid, device allocation, upload, first lists and force; steps; copy back)."""
+        lib.md_set_precision(precision)
+        runs = []
+        for rep in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s = tm.Simulation(lib, m, x, v, world_box, rank_box, temp=1.44)
+            lib.md_synchronize()
+            ta = time.perf_counter()
+            s.run(DT, K)
+            lib.md_synchronize()
+            tb = time.perf_counter()
+            s.arrays()  # md_copy_data_from_accelerator + md_write_grid_data_to_arrays
+            t1 = time.perf_counter()
+            s.close()
+            runs.append((t1 - t0, ta - t0, tb - ta, t1 - tb))
+        lib.md_set_precision(0)
+        return min(runs)
+
+    best = e2e_best(1)
+    best64 = e2e_best(0)
     e2e_value, e2e_ms = replica_rate(natoms, world, K, best[0] * 1e3, dist, dev)
-    lib.md_set_precision(0)
-    h2d = natoms * (8 + 24 + 24)
-    d2h = (natoms + nghost) * (32 * 3 + 16 + 8 + 4)  # md_copy_data_from_accelerator
+    e2e_value64, _ = replica_rate(natoms, world, K, best64[0] * 1e3, dist, dev)
+    h2d = natoms * (8 + 24 + 24)  # masses, positions, velocities up
+    d2h = natoms * (8 + 24 + 24 + 24)  # the locals' masses, positions, velocities, forces down
 
     peak, peak_kind = peaks()
     force_ms = fms.value / max(nl.value, 1)
@@ -525,6 +576,10 @@ def run_ours(args):
                   "mixed_max_force_err_over_rms": ferr, "mixed_energy_err": eerr},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
+                     # what the ncu capture of this kernel shows limits it (profiles/lj_mixed_full_131k_ncu.md)
+                     "limiter": "instruction issue and latency, not HBM: ncu issue active 58 %, DRAM 19 % of peak, "
+                                "gathers served by L1 (75 % hit) and L2",
+                     "traffic_frac": (traffic / (force_ms * 1e-3) / 1e9 / peak) if traffic else None,
                      "bytes_per_atom": bytes_per_atom, "force_bytes_per_atom": force_bytes,
                      "integrate_ghost_bytes_per_atom": step_bytes, "mean_list_length": mean_nb,
                      "launch_ms": force_ms, "launches_timed": nl.value, "timed_every": PROFILE_EVERY,
@@ -537,10 +592,13 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
                 "note": "md_initialize_grid from host arrays .. K steps .. md_write_grid_data_to_arrays, host clock",
-                "setup_ms": best[1] * 1e3, "steps_ms": best[2] * 1e3, "copy_back_ms": best[3] * 1e3},
+                "setup_ms": best[1] * 1e3, "steps_ms": best[2] * 1e3, "copy_back_ms": best[3] * 1e3,
+                "fp64": {"value": e2e_value64, "setup_ms": best64[1] * 1e3, "steps_ms": best64[2] * 1e3,
+                         "copy_back_ms": best64[3] * 1e3}},
         "drift": drift,
         "adjoint": adj,
         "workloads": more,
+        "kernels": ktable,
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
@@ -567,18 +625,43 @@ import ctypes  # noqa: E402
 
 
 def profile_case(args):
-    """The benchmark workload in one form for `args.steps` steps, untimed (an ncu target)."""
+    """One workload in one form for `args.steps` steps, untimed (an ncu target):
+    mixed / fp64 [_half]   the 131k LJ workload (full lists, or half lists keeping boundary pairs)
+    mixed_c2 / fp64_c2     the 'half' setup at 64^3 (524,288 atoms), full lists
+    dem_mixed / dem_fp64   DEM at 48^3, FCC diagonal split, contact-fixed model (R = 0.6)
+    adjoint                the differentiable form: 16^3 cells, one forward and one backward pass"""
     import tinymd as tm
     lib = tm.load()
-    half = args.profile_case.endswith("_half")
-    lib.md_set_precision(1 if args.profile_case.startswith("mixed") else 0)
-    if half:
-        lib.md_set_half_mode(1)
-        lib.md_set_ghost_mode(1)
-    sim = tm.Simulation(lib, *tm.setup_particles("default", CELLS, lib=lib), temp=1.44, half=half)
-    sim.run(DT, args.steps)
-    sim.close()
-    print(f"profile case {args.profile_case}: {args.steps} steps, error code {lib.md_last_error()}")
+    case = args.profile_case
+    if case == "adjoint":
+        import torch
+        from tinymd import adjoint
+        parts = tm.setup_particles("default", (16, 16, 16), lib=lib)
+        sim = tm.Simulation(lib, *parts, temp=1.44)
+        v0 = adjoint.initial_velocities(lib, sim)
+        adjoint.configure(lib, steps=args.steps, reneigh=20, dt=DT, precision=1, shifted_energy=True)
+        v = torch.tensor(v0, requires_grad=True)
+        e = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+        sg = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+        adjoint.TrajectoryLoss.apply(v, e, sg, lib).backward()
+        sim.close()
+    else:
+        lib.md_set_precision(1 if case.startswith("mixed") or case == "dem_mixed" else 0)
+        half = case.endswith("_half")
+        if half:
+            lib.md_set_half_mode(1)
+            lib.md_set_ghost_mode(1)
+        if case.startswith("dem"):
+            lib.md_set_dem_model(1, 0.6)
+            parts = tm.setup_particles("granular_gas_fcc", (48, 48, 48), lib=lib)
+            sim = tm.Simulation(lib, *parts, force_field="dem", dem=(0.1, 0.1, 100.0, 0.5), cutoff=1.2)
+            sim.run(0.001, args.steps)
+        else:
+            cells, setup = ((64, 64, 64), "half") if case.endswith("_c2") else (CELLS, "default")
+            sim = tm.Simulation(lib, *tm.setup_particles(setup, cells, lib=lib), temp=1.44, half=half)
+            sim.run(DT, args.steps)
+        sim.close()
+    print(f"profile case {case}: {args.steps} steps, error code {lib.md_last_error()}")
     return 0 if lib.md_last_error() == 0 else 1
 
 
@@ -589,7 +672,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--profile-case", choices=["mixed", "fp64", "mixed_half", "fp64_half"],
+    ap.add_argument("--profile-case", choices=["mixed", "fp64", "mixed_half", "fp64_half", "mixed_c2", "fp64_c2",
+                                               "dem_mixed", "dem_fp64", "adjoint"],
                     help="run the workload for --steps steps in one form and exit (for ncu captures)")
     args = ap.parse_args()
     if args.profile_case:

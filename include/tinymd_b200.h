@@ -171,6 +171,12 @@ void md_set_thermo(int enable);
  * list entries inside the cutoff, out[3] = sum of v.v of locals after the last
  * final integration.  Full lists count each pair twice. Returns 0 on success. */
 int md_get_thermo(double *out);
+/* The same sums without waiting: md_thermo_request enqueues a copy of them (as of the work
+ * issued so far) into page-locked memory and returns a ticket; md_thermo_fetch(ticket, out)
+ * waits for that copy alone and fills out[4] as md_get_thermo does.  Up to 8 requests stay
+ * fetchable; returns 0, or -1 for an unknown ticket. */
+int md_thermo_request(void);
+int md_thermo_fetch(int ticket, double *out);
 /* Blocks until all enqueued device work is done. */
 void md_synchronize(void);
 /* Use `stream` (a cudaStream_t) for all library work instead of the stream

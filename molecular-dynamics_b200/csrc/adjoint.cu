@@ -444,6 +444,7 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
         hx[i] = make_double4(s.h_x0[3 * i], s.h_x0[3 * i + 1], s.h_x0[3 * i + 2], 0.0);
         hv[i] = make_double4(v0[3 * i], v0[3 * i + 1], v0[3 * i + 2], 0.0);
     }
+    materialize_mirror(s);
     std::vector<double> hm(s.h_mass.begin(), s.h_mass.begin() + N);
     TMD_CUDA(cudaMemcpyAsync(x0_dev, hx.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
     TMD_CUDA(cudaMemcpyAsync(ck_x, hx.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));

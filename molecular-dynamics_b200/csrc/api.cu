@@ -252,6 +252,11 @@ void free_all(State& s) {
         cudaEventDestroy(s.ev_counted);
         s.ev_counted = nullptr;
     }
+    for (int k = 0; k < kThermoSlots; ++k) {
+        if (s.thermo_ev[k]) cudaEventDestroy(s.thermo_ev[k]);
+        s.thermo_ev[k] = nullptr;
+        s.thermo_slot_ticket[k] = -1;
+    }
     dfree(&s.thermo_dev);
     dfree(&s.status_dev);
     s.scan_part_cap = 0;
@@ -264,6 +269,7 @@ void free_all(State& s) {
 // grows every per-slot array to hold `need` slots, keeping contents; false (error latched,
 // arrays unchanged) when the device has no room
 bool grow_atoms(State& s, int need) {
+    if (s.mirror_pending) materialize_mirror(s);  // dl_buf is carved from the slab
     const int oldc = s.capA;
     // a multiple of 64 slots: per-slot planes laid out back to back (img_slot) start on
     // 256-byte boundaries, as bulk prefetches need
@@ -324,7 +330,12 @@ bool allocate_state(State& s, int N, int nb_cap) {
     dalloc(&s.thermo_dev, 8);
     dalloc(&s.status_dev, 1);
     if (!s.status_host) TMD_CUDA(cudaMallocHost((void**)&s.status_host, sizeof(DevStatus)));
-    if (!s.thermo_host) TMD_CUDA(cudaMallocHost((void**)&s.thermo_host, 8 * sizeof(double)));
+    if (!s.thermo_host) TMD_CUDA(cudaMallocHost((void**)&s.thermo_host, kThermoSlots * 4 * sizeof(double)));
+    for (int k = 0; k < kThermoSlots; ++k) {
+        if (!s.thermo_ev[k]) TMD_CUDA(cudaEventCreateWithFlags(&s.thermo_ev[k], cudaEventDisableTiming));
+        s.thermo_slot_ticket[k] = -1;
+    }
+    s.thermo_tickets = 0;
     TMD_CUDA(cudaMemsetAsync(s.status_dev, 0, sizeof(DevStatus), s.stream));
     TMD_CUDA(cudaMemsetAsync(s.thermo_dev, 0, 8 * sizeof(double), s.stream));
     ensure_scan_scratch(s, std::max(nseg, 26 * nblk));
@@ -538,6 +549,32 @@ double host_temperature(const State& s) {  // core/thermo.impala:1-16 on the hos
 }
 
 }  // namespace
+
+// copies of the snapshot in dl_buf ([mass NA][pos 3NA][vel 3NA][frc 3NA], reference order):
+// rows [r0, r1) of each array into the given destinations
+static void copy_snapshot(State& s, int r0, int r1, double* m, double* x, double* v, double* f) {
+    const size_t na = (size_t)s.mirror_na, a = (size_t)r0, n = (size_t)(r1 - r0);
+    if (n == 0) return;
+    TMD_CUDA(cudaMemcpyAsync(m, s.dl_buf + a, sizeof(double) * n, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(x, s.dl_buf + na + 3 * a, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, s.stream));
+    TMD_CUDA(cudaMemcpyAsync(v, s.dl_buf + 4 * na + 3 * a, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                             s.stream));
+    TMD_CUDA(cudaMemcpyAsync(f, s.dl_buf + 7 * na + 3 * a, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+                             s.stream));
+}
+
+void materialize_mirror(State& s, int parts) {
+    const int todo = s.mirror_pending & parts;
+    if (!todo) return;
+    const int n = s.mirror_n, na = s.mirror_na;
+    if (todo & 1) copy_snapshot(s, 0, n, s.h_mass.data(), s.h_pos.data(), s.h_vel.data(), s.h_frc.data());
+    if (todo & 2)
+        copy_snapshot(s, n, na, s.h_mass.data() + n, s.h_pos.data() + 3 * (size_t)n, s.h_vel.data() + 3 * (size_t)n,
+                      s.h_frc.data() + 3 * (size_t)n);
+    TMD_CUDA(cudaStreamSynchronize(s.stream));
+    s.mirror_pending &= ~todo;
+}
+
 }  // namespace tmd
 
 using namespace tmd;
@@ -610,6 +647,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.pend_force = PendingForce();
     s.pend_final = s.pend_ghost = s.pend_kick = s.pend_pbc = false;
     s.bin_zeroed = s.build_zeroed = s.pend_links = false;
+    s.mirror_pending = 0;
     s.force_iters = s.rsq_iters = s.integration_iters = 0;
     s.launches = 0;
     if (!allocate_state(s, n, neighborlist_capacity)) {
@@ -640,6 +678,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
 void md_create_velocity(double t_request) {
     State& s = g_state;
     if (!require_alive("md_create_velocity")) return;
+    materialize_mirror(s);
     const int n = s.N;
     double vt[3] = {0.0, 0.0, 0.0};
     for (int i = 0; i < n; ++i)
@@ -658,6 +697,7 @@ void md_copy_data_to_accelerator(void) {
     State& s = g_state;
     if (!require_alive("md_copy_data_to_accelerator")) return;
     flush_all(s);
+    materialize_mirror(s);  // the upload goes through dl_buf
     const int N = s.N;
     s.G = 0;
     s.pc = s.vc = s.ac = 0;
@@ -677,32 +717,29 @@ void md_copy_data_to_accelerator(void) {
     sync_stream(s);
 }
 
-// core/grid.impala:369-374: device -> host mirror, scattered to reference order
+// core/grid.impala:369-374: device -> host mirror, scattered to reference order.  The state is
+// gathered into reference order on the device now (the snapshot); the copy to the host happens
+// when a reader needs it, and then only the part it needs: md_write_grid_data_to_arrays takes
+// the locals straight into the caller's arrays.
 void md_copy_data_from_accelerator(void) {
     State& s = g_state;
     if (!require_alive("md_copy_data_from_accelerator")) return;
     flush_all(s);
     const int NA = s.N + s.G;
-    // every element is overwritten below (the gather covers all NA reference indices)
+    // every element is overwritten when the pending parts are copied (all NA reference indices)
     s.h_mass.resize(NA);
     s.h_pos.resize((size_t)NA * 3);
     s.h_vel.resize((size_t)NA * 3);
     s.h_frc.resize((size_t)NA * 3);
+    s.mirror_pending = 0;
     if (NA == 0) return;
-    // gathered into reference order on the device, copied straight into the page-locked mirror
     k_gather_ref<<<(NA + 255) / 256, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.frc32,
                                                          s.mass.b[s.ac], s.ref.b[s.ac], s.dl_buf, s.N, NA,
                                                          s.precision == 1, s.dem_fixed);
     launched(K_MISC);
-    const size_t na = (size_t)NA;
-    TMD_CUDA(cudaMemcpyAsync(s.h_mass.data(), s.dl_buf, sizeof(double) * na, cudaMemcpyDeviceToHost, s.stream));
-    TMD_CUDA(cudaMemcpyAsync(s.h_pos.data(), s.dl_buf + na, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost,
-                             s.stream));
-    TMD_CUDA(cudaMemcpyAsync(s.h_vel.data(), s.dl_buf + 4 * na, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost,
-                             s.stream));
-    TMD_CUDA(cudaMemcpyAsync(s.h_frc.data(), s.dl_buf + 7 * na, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost,
-                             s.stream));
-    sync_stream(s);
+    s.mirror_pending = (s.N > 0 ? 1 : 0) | (s.G > 0 ? 2 : 0);
+    s.mirror_n = s.N;
+    s.mirror_na = NA;
 }
 
 void md_exchange_particles(void) {  // comm/comm.impala:392-525: no remote ranks in one process
@@ -876,6 +913,13 @@ int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* 
     State& s = g_state;
     if (!require_alive("md_write_grid_data_to_arrays")) return 0;
     flush_all(s);
+    if ((s.mirror_pending & 1) && s.mirror_n == s.N) {  // the snapshot's locals, straight to the caller
+        copy_snapshot(s, 0, s.N, m, reinterpret_cast<double*>(x), reinterpret_cast<double*>(v),
+                      reinterpret_cast<double*>(f));
+        TMD_CUDA(cudaStreamSynchronize(s.stream));
+        return s.N;
+    }
+    materialize_mirror(s);
     const size_t n = std::min((size_t)s.N, s.h_mass.size());
     if (n > 0) {
         std::memcpy(m, s.h_mass.data(), sizeof(double) * n);
@@ -891,6 +935,13 @@ int md_write_grid_ghost_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vect
     State& s = g_state;
     if (!require_alive("md_write_grid_ghost_data_to_arrays")) return 0;
     flush_all(s);
+    if ((s.mirror_pending & 2) && s.mirror_n == s.N && s.mirror_na == s.N + s.G) {  // straight to the caller
+        copy_snapshot(s, s.N, s.N + s.G, m, reinterpret_cast<double*>(x), reinterpret_cast<double*>(v),
+                      reinterpret_cast<double*>(f));
+        TMD_CUDA(cudaStreamSynchronize(s.stream));
+        return s.N;
+    }
+    materialize_mirror(s);
     const size_t have = s.h_mass.size();
     const size_t n0 = (size_t)s.N;
     const size_t ng = have > n0 ? std::min((size_t)s.G, have - n0) : 0;
@@ -929,6 +980,7 @@ void md_deallocate_grid(void) {
     fold_prof(true);
     phase_reset();
     free_all(s);
+    s.mirror_pending = 0;
     s.alive = false;
     s.N = s.G = 0;
     s.capA = 0;
@@ -937,6 +989,7 @@ void md_deallocate_grid(void) {
 // core/runtime.impala:146-156 (host mirror)
 void md_print_grid(void) {
     State& s = g_state;
+    if (s.alive) materialize_mirror(s);
     for (int i = 0; i < s.N; ++i) {
         std::printf("0> pos_local: ");
         print_g(s.h_pos[3 * i]); std::printf(", "); print_g(s.h_pos[3 * i + 1]); std::printf(", ");
@@ -952,6 +1005,7 @@ void md_print_grid(void) {
 
 void md_print_ghost(void) {
     State& s = g_state;
+    if (s.alive) materialize_mirror(s);
     const size_t have = s.h_mass.size();
     for (int i = s.N; i < s.N + s.G && (size_t)i < have; ++i) {
         std::printf("0> pos_ghost: ");
@@ -1062,7 +1116,10 @@ void md_report_iterations(void) {
 // core/runtime.impala:298-316 (temperature from the host mirror)
 void md_report_particles(void) {
     State& s = g_state;
-    if (s.alive) flush_all(s);
+    if (s.alive) {
+        flush_all(s);
+        materialize_mirror(s, 1);
+    }
     std::printf("# Local # Ghost Temp\n");
     std::printf("%d %d ", s.N, s.G);
     print_g(host_temperature(s));
@@ -1122,6 +1179,34 @@ int md_get_thermo(double* out) {
     flush_all(s);
     TMD_CUDA(cudaMemcpyAsync(out, s.thermo_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     sync_stream(s);
+    s.rsq_iters = (long long)out[2];
+    return 0;
+}
+// Asynchronous thermo: the sums as of the work enqueued so far go to a page-locked slot by a
+// copy on the library stream, gated by an event; nothing waits until the ticket is fetched.
+int md_thermo_request(void) {
+    State& s = g_state;
+    if (!require_alive("md_thermo_request")) return -1;
+    flush_all(s);
+    const long long t = s.thermo_tickets++;
+    const int k = (int)(t % kThermoSlots);
+    if (s.thermo_slot_ticket[k] >= 0) TMD_CUDA(cudaEventSynchronize(s.thermo_ev[k]));  // slot reused
+    TMD_CUDA(cudaMemcpyAsync(s.thermo_host + 4 * k, s.thermo_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                             s.stream));
+    TMD_CUDA(cudaEventRecord(s.thermo_ev[k], s.stream));
+    s.thermo_slot_ticket[k] = t;
+    return (int)t;
+}
+int md_thermo_fetch(int ticket, double* out) {
+    State& s = g_state;
+    if (!require_alive("md_thermo_fetch")) return -1;
+    const int k = ticket >= 0 ? ticket % kThermoSlots : 0;
+    if (ticket < 0 || s.thermo_slot_ticket[k] != ticket) {
+        set_error(MD_ERR_ARGUMENT, "md_thermo_fetch: unknown ticket (more than 8 requests since, or none)");
+        return -1;
+    }
+    TMD_CUDA(cudaEventSynchronize(s.thermo_ev[k]));
+    for (int q = 0; q < 4; ++q) out[q] = s.thermo_host[4 * k + q];
     s.rsq_iters = (long long)out[2];
     return 0;
 }

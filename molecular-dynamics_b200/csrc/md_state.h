@@ -109,6 +109,8 @@ constexpr int kImg1 = 6;
 constexpr int kImg2 = 8;
 constexpr int kImgW = kImg1 + kImg2;
 
+constexpr int kThermoSlots = 8;  // asynchronous thermo reads in flight at most
+
 struct PendingForce {
     bool valid = false;
     bool dem = false;
@@ -193,9 +195,18 @@ struct State {
     DevStatus* status_host = nullptr;  // pinned
     cudaEvent_t ev_counted = nullptr;  // the ghost count's readback (run_borders)
     int scan_attr_device = -1;         // device whose k_scan_single shared-memory attribute is set
-    double* thermo_host = nullptr;     // pinned [8]
+    double* thermo_host = nullptr;     // pinned [kThermoSlots][4]: asynchronous thermo reads
+    cudaEvent_t thermo_ev[8] = {};     // one per slot: its copy has landed
+    long long thermo_slot_ticket[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
+    long long thermo_tickets = 0;      // tickets issued by md_thermo_request
 
     // host mirror in reference order (core/grid.impala ArrayData host buffers)
+    // md_copy_data_from_accelerator gathers the device state into dl_buf and leaves the copy
+    // to the host pending: bit 0 the locals, bit 1 the ghosts of that snapshot (mirror_n locals,
+    // mirror_na slots).  Readers copy what they need; anything that would overwrite dl_buf
+    // first completes the mirror (materialize_mirror).
+    int mirror_pending = 0;
+    int mirror_n = 0, mirror_na = 0;
     HostVec h_mass;                 // [N+G]
     HostVec h_pos, h_vel, h_frc;    // [(N+G)*3]
     HostVec h_x0;                   // initial positions (adjoint)
@@ -266,6 +277,9 @@ void run_integrate(State& s, double dt, bool fuse_ghosts, double kick_dt = -1.0)
 void run_ghost_sync(State& s);
 void run_final(State& s, double dt);
 void run_refresh_pos32(State& s);
+// completes the pending host-mirror copies of the last md_copy_data_from_accelerator (parts:
+// bit 0 locals, bit 1 ghosts)
+void materialize_mirror(State& s, int parts = 3);
 // list pairs inside the cutoff rc (FP64), the reference's rsq_iters of a force call on the
 // current lists and positions
 long long count_pairs_inside(State& s, double rc);

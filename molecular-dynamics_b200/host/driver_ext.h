@@ -34,6 +34,19 @@ inline void thermo(double* out) {
     int n = md_get_number_of_particles();
     out[2] = oracle_temperature() * (3.0 * n - 3.0);
 }
+// the oracle runs synchronously: a request takes the sums at once and a fetch returns them
+inline double* thermo_ring() {
+    static double ring[8][3];
+    return &ring[0][0];
+}
+inline int thermo_request() {
+    static int t = 0;
+    thermo(thermo_ring() + 3 * (t % 8));
+    return t++;
+}
+inline void thermo_fetch(int ticket, double* out) {
+    for (int q = 0; q < 3; ++q) out[q] = thermo_ring()[3 * (ticket % 8) + q];
+}
 inline bool phase_times(double*) { return false; }
 inline void enable_phase_timing() {}
 inline const char* backend() { return "cpu oracle (restatement of the reference cpu backend)"; }
@@ -51,6 +64,15 @@ inline void set_thermo(int on) { md_set_thermo(on); }
 inline void thermo(double* out) {
     double t[4];
     md_get_thermo(t);
+    out[0] = t[0];
+    out[1] = t[1];
+    out[2] = t[3];
+}
+// the sums go to page-locked memory behind the enqueued work; fetching waits for that copy only
+inline int thermo_request() { return md_thermo_request(); }
+inline void thermo_fetch(int ticket, double* out) {
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    md_thermo_fetch(ticket, t);
     out[0] = t[0];
     out[1] = t[1];
     out[2] = t[3];

@@ -143,9 +143,7 @@ void vtk_dump(const std::string& dir, int step) {
 
 // thermo line: step, temperature (dof 3N-3), potential energy per atom,
 // pressure, total energy per atom (extension; the reference prints none)
-void thermo_line(int step, bool half_nb, double volume) {
-    double t[3];
-    drv::thermo(t);
+void print_thermo(int step, const double* t, bool half_nb, double volume) {
     const int n = md_get_number_of_particles();
     const double w = half_nb ? 1.0 : 0.5;
     const double epot = t[0] * w, vir = t[1] * w;
@@ -155,6 +153,28 @@ void thermo_line(int step, bool half_nb, double volume) {
     std::printf("thermo %d %.9e %.9e %.9e %.9e\n", step, temp, epot / n, press, (0.5 * t[2] + epot) / n);
     std::fflush(stdout);
 }
+
+// Thermo lines without stalling the timestep loop: a line's sums are requested when its step
+// is enqueued (a copy into page-locked memory behind that step's work) and printed one thermo
+// interval later, when the copy has long landed; the last line is printed after the loop.
+struct ThermoLines {
+    bool half_nb = false;
+    double volume = 1.0;
+    int pending_step = -1, pending_ticket = -1;
+    void request(int step) {
+        const int ticket = drv::thermo_request();
+        flush();
+        pending_step = step;
+        pending_ticket = ticket;
+    }
+    void flush() {
+        if (pending_step < 0) return;
+        double t[3];
+        drv::thermo_fetch(pending_ticket, t);
+        print_thermo(pending_step, t, half_nb, volume);
+        pending_step = -1;
+    }
+};
 
 }  // namespace
 
@@ -348,9 +368,12 @@ int main(int argc, char** argv) {
             else md_compute_lennard_jones(half_nb, cutoff, epsilon, sigma);
         };
         force();
+        ThermoLines thermo;
+        thermo.half_nb = half_nb;
+        thermo.volume = volume;
         if (thermo_every > 0) {
             md_final_integration(0.0);  // a zero kick: drains the force and reduces v.v
-            thermo_line(0, half_nb, volume);
+            thermo.request(0);
         }
         if (vtk && run == 0) {
             md_copy_data_from_accelerator();
@@ -382,8 +405,7 @@ int main(int argc, char** argv) {
             force();
             md_final_integration(dt);
             timer.accum(T_FORCE);
-            if (thermo_every > 0 && ((j + 1) % thermo_every == 0 || j + 1 == steps))
-                thermo_line(j + 1, half_nb, volume);
+            if (thermo_every > 0 && ((j + 1) % thermo_every == 0 || j + 1 == steps)) thermo.request(j + 1);
             if (vtk && run == 0) {
                 md_copy_data_from_accelerator();
                 vtk_dump(vtk_dir, j + 1);
@@ -391,6 +413,7 @@ int main(int argc, char** argv) {
             }
         }
         md_barrier();
+        thermo.flush();
         timer.accum(T_OTHER);
         auto w1 = Clock::now();
         timer.finish();

@@ -69,6 +69,8 @@ _EXTENSION_API = {
     "md_set_dem_model": (None, [_c_int, _c_double]),
     "md_set_thermo": (None, [_c_int]),
     "md_get_thermo": (_c_int, [_vp]),
+    "md_thermo_request": (_c_int, []),
+    "md_thermo_fetch": (_c_int, [_c_int, _vp]),
     "md_synchronize": (None, []),
     "md_set_stream": (None, [_vp]),
     "md_get_phase_times": (None, [_vp]),
