@@ -107,7 +107,9 @@ __device__ __forceinline__ int reaction_slot(int j, int N, const int* groot) { r
 
 // ---- FP64 LJ ------------------------------------------------------------------
 #ifndef TMD_MINB
-#define TMD_MINB (1024 / TMD_THREADS)  // caps registers at 64 per thread
+// seven 128-thread blocks per SM cap registers at 72 per thread, and 7 x 148 blocks still hold the
+// 1,024 blocks of 131k atoms in one wave (the mixed kernel: 37.4 -> 36.9 us against 64 registers)
+#define TMD_MINB 7
 #endif
 // v += dt/2 f; x += dt v (core/compute.impala:97-106) in the reference's operand order
 __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, double fx, double fy, double fz,
@@ -121,6 +123,15 @@ __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, d
 constexpr int kB64 = 4;  // neighbours per batch (FP64): one list quad
 constexpr int kB32 = 4;  // neighbours per batch (mixed): one list quad
 constexpr int kQ = 8;    // FP64-path neighbours a mixed thread queues before working them off
+// TMD_MX_LEAN: f = sr2 sr6 (48 eps sr6 - 24 eps), one operation fewer per pair.
+// TMD_MX_SLOWPRED: FP64-path pairs queued without a branch (measured with 72 registers:
+// 37.4 -> 35.4 us together with the lean formula; with 64 registers it spilled, 48 us).
+#ifndef TMD_MX_LEAN
+#define TMD_MX_LEAN 1
+#endif
+#ifndef TMD_MX_SLOWPRED
+#define TMD_MX_SLOWPRED 1
+#endif
 
 // Ghost images written by the force kernel that integrates (maps from k_ghost_links): each
 // local writes the ghosts that are its images, from its new position, and extra threads
@@ -468,6 +479,16 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
             for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (cur[u] >> kCodeBits));
             // the next quad loads while this one's gathers are in flight
             eq = list_quad(nbl, min(b + 1, nquad - 1), i, a.stride);
+#if TMD_MX_SLOWPRED
+            // room for this quad's FP64 pairs in the queue (rarely short: worked off first)
+            if (__any_sync(__activemask(), nq > kQ - kB32)) {
+                if (nq > kQ - kB32) {
+                    const double4 pi = ldg_d4(pos + i);
+                    for (int q = 0; q < nq; ++q) fp64_lj<THERMO>(pi, s_q[q][threadIdx.x], pos, a, cx, cy, cz, e, w, ncnt);
+                    nq = 0;
+                }
+            }
+#endif
             unsigned slow = 0;
 #pragma unroll
             for (int u = 0; u < kB32; ++u) {
@@ -480,11 +501,23 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
                 const float dz = fmaf(a.hz, sz, ri.z - rj[u].z);
                 const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const bool fast = rsq < a.rc2_lo && rsq >= a.close2;
+#if TMD_MX_SLOWPRED
+                {  // queued without a branch: the slot is written always, counted only for FP64 pairs
+                    const bool sl = !fast && rsq < a.rc2_hi;
+                    s_q[nq][threadIdx.x] = (int)(en >> kCodeBits);
+                    nq += sl ? 1 : 0;
+                }
+#else
                 slow |= (!fast && rsq < a.rc2_hi) ? (1u << u) : 0u;
+#endif
                 float sr2;
                 asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
                 const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
+#if TMD_MX_LEAN
+                float f = sr6 * sr2 * fmaf(a.eps48f, sr6, a.eps24nf);
+#else
                 float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
+#endif
                 f = fast ? f : 0.f;
                 fx = fmaf(dx, f, fx);
                 fy = fmaf(dy, f, fy);
@@ -495,6 +528,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
                     ncnt += fast ? 1 : 0;
                 }
             }
+#if !TMD_MX_SLOWPRED
             while (slow) {  // queued in list order; a full queue is worked off first (rare)
                 const int u = __ffs(slow) - 1;
                 slow &= slow - 1u;
@@ -506,6 +540,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
                 }
                 s_q[nq++][threadIdx.x] = (int)(en >> kCodeBits);
             }
+#endif
         }
         // the FP64 pairs of the whole list, worked off together: the warp's lanes run them side
         // by side instead of one lane at a time inside the loop

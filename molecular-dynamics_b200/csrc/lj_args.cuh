@@ -12,7 +12,7 @@ struct LjArgs {
     double dt_i, h_i;          // the next step's initial integration (fused kernels only)
     double alo[3], rb_h;       // rebasing grid (mixed form's positions)
     // mixed form
-    float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f;
+    float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f, eps24nf;
     float hx, hy, hz;  // shift decode scales (see the kernels)
 };
 
@@ -54,6 +54,7 @@ inline LjArgs lj_args(const State& s, const PendingForce& p, double dt) {
     a.close2 = (float)((1.04 * p.sigma) * (1.04 * p.sigma));
     a.sig6f = (float)a.sigma6;
     a.eps48f = (float)(48.0 * p.eps);
+    a.eps24nf = (float)(-24.0 * p.eps);
     a.eps4f = (float)(4.0 * p.eps);
     a.hx = a.hy = a.hz = 0.0f;
     return a;
