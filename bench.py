@@ -8,8 +8,10 @@ full neighbour lists.  A "step" is one MD timestep (main.cpp:715-776).
 
 value   atom-steps/s of the mixed form (FP64 state / FP32 pair forces) over K
         device-timed steps (CUDA events around each step on the library's
-        stream; the 131k working set fits in L2, so L2 is flushed by writing a
-        256 MiB buffer before every timed step, outside the timed interval).
+        stream; the 131k working set fits in L2, so L2 is flushed before every
+        timed step, outside the timed interval, by writing a 256 MiB buffer and
+        reading it back: the step starts cold and without the flush's dirty
+        lines to write back).
 forms   the FP64 form's atom-steps/s on the same workload, the ratio, and the
         mixed form's max force error / rms force against FP64 positions.
 e2e     the same metric through the C ABI with host buffers: md_initialize_grid
@@ -570,7 +572,9 @@ def run_ours(args):
         "dtype": "f64 state + f32 pair forces (mixed form)",
         "data": "synthetic (seeded FCC lattice, reference Park-Miller velocities)",
         "config": {"workload": "lj_default_fcc_32x32x32_131072_atoms_full_list", "atoms_per_gpu": natoms,
-                   "dt": DT, "reneigh": 20, "cutoff": 2.5, "skin": 0.3, "l2": "flushed before every timed step",
+                   "dt": DT, "reneigh": 20, "cutoff": 2.5, "skin": 0.3,
+                   "l2": "flushed before every timed step: a 256 MiB buffer written, then read back (the read "
+                         "evicts the written lines), outside the timed interval",
                    "parallelism": f"replicas x{world}"},
         "forms": {"mixed": value, "fp64": value64, "mixed_over_fp64": value / value64,
                   "mixed_max_force_err_over_rms": ferr, "mixed_energy_err": eerr},

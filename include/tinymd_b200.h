@@ -207,8 +207,10 @@ long long md_device_bytes(void);
  * `list_cutoff` -- then the force of the last md_compute_* call and the final
  * integration.  When step_ms is not NULL each step is bracketed by CUDA
  * events and its device time stored; when flush_buf is not NULL, flush_bytes
- * of it are overwritten before each step, outside the timed interval (an L2
- * flush for benchmarking).  Returns 0 on success. */
+ * of it are overwritten and then read back before each step, outside the
+ * timed interval (an L2 flush for benchmarking: the read evicts the written
+ * lines, so the step starts with a cold L2 that holds no dirty lines of the
+ * flush).  Returns 0 on success. */
 int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double list_cutoff, float *step_ms,
                      void *flush_buf, long long flush_bytes);
 
