@@ -439,12 +439,13 @@ int md_adjoint_forward(double const* v0, double epsilon, double sigma, double* l
     dfree(&mass_ref);
     dalloc(&mass_ref, N);
     // initial state in reference order: x_0 from md_initialize_grid, v_0 from the caller
+    materialize_mirror(s);
+    const double* x0 = s.x0_in_pos ? s.h_pos.data() : s.h_x0.data();
     std::vector<double4> hx(N), hv(N);
     for (int i = 0; i < N; ++i) {
-        hx[i] = make_double4(s.h_x0[3 * i], s.h_x0[3 * i + 1], s.h_x0[3 * i + 2], 0.0);
+        hx[i] = make_double4(x0[3 * i], x0[3 * i + 1], x0[3 * i + 2], 0.0);
         hv[i] = make_double4(v0[3 * i], v0[3 * i + 1], v0[3 * i + 2], 0.0);
     }
-    materialize_mirror(s);
     std::vector<double> hm(s.h_mass.begin(), s.h_mass.begin() + N);
     TMD_CUDA(cudaMemcpyAsync(x0_dev, hx.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));
     TMD_CUDA(cudaMemcpyAsync(ck_x, hx.data(), sizeof(double4) * N, cudaMemcpyHostToDevice, s.stream));

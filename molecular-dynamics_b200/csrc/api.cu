@@ -567,6 +567,11 @@ void materialize_mirror(State& s, int parts) {
     const int todo = s.mirror_pending & parts;
     if (!todo) return;
     const int n = s.mirror_n, na = s.mirror_na;
+    if ((todo & 1) && s.x0_in_pos) {  // the initial positions are about to be overwritten
+        s.h_x0.assign(s.h_pos.begin(), s.h_pos.begin() + 3 * (size_t)n);
+        s.x0_in_pos = false;
+    }
+    if (todo & 1) s.mirror_frc_zero = false;
     if (todo & 1) copy_snapshot(s, 0, n, s.h_mass.data(), s.h_pos.data(), s.h_vel.data(), s.h_frc.data());
     if (todo & 2)
         copy_snapshot(s, n, na, s.h_mass.data() + n, s.h_pos.data() + 3 * (size_t)n, s.h_vel.data() + 3 * (size_t)n,
@@ -661,14 +666,15 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     s.h_pos.resize((size_t)n * 3);
     s.h_vel.resize((size_t)n * 3);
     s.h_frc.resize((size_t)n * 3);
-    s.h_x0.resize((size_t)n * 3);
     if (n > 0) {
         std::memcpy(s.h_mass.data(), masses, sizeof(double) * n);
         std::memcpy(s.h_pos.data(), positions, sizeof(Vector3D) * n);
         std::memcpy(s.h_vel.data(), velocities, sizeof(Vector3D) * n);
-        std::memset(s.h_frc.data(), 0, sizeof(Vector3D) * n);
-        std::memcpy(s.h_x0.data(), positions, sizeof(Vector3D) * n);
     }
+    // the mirror's forces are zero (written out as zeros until a snapshot fills them) and the
+    // initial positions are the mirror's until a snapshot overwrites them (kept aside then)
+    s.mirror_frc_zero = true;
+    s.x0_in_pos = true;
     s.alive = true;
     phase_reset();
     return s.N;
@@ -684,9 +690,15 @@ void md_create_velocity(double t_request) {
     for (int i = 0; i < n; ++i)
         for (int d = 0; d < 3; ++d) vt[d] = vt[d] + s.h_vel[3 * i + d];
     for (int d = 0; d < 3; ++d) vt[d] = vt[d] / (double)n;
-    for (int i = 0; i < n; ++i)
-        for (int d = 0; d < 3; ++d) s.h_vel[3 * i + d] = s.h_vel[3 * i + d] - vt[d];
-    double t = host_temperature(s);
+    // the mean removed and core/thermo.impala:1-16's sum taken in the same pass (same terms in
+    // the same order as a separate pass over the updated velocities)
+    double t = 0.0;
+    for (int i = 0; i < n; ++i) {
+        double* v = &s.h_vel[(size_t)i * 3];
+        for (int d = 0; d < 3; ++d) v[d] = v[d] - vt[d];
+        t += (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * 1.0;
+    }
+    t = t * (1.0 / (double)(n * 3 - 3));
     double factor = std::sqrt(t_request / t);
     for (int i = 0; i < n; ++i)
         for (int d = 0; d < 3; ++d) s.h_vel[3 * i + d] = s.h_vel[3 * i + d] * factor;
@@ -925,7 +937,8 @@ int md_write_grid_data_to_arrays(double* m, Vector3D* x, Vector3D* v, Vector3D* 
         std::memcpy(m, s.h_mass.data(), sizeof(double) * n);
         std::memcpy(x, s.h_pos.data(), sizeof(Vector3D) * n);
         std::memcpy(v, s.h_vel.data(), sizeof(Vector3D) * n);
-        std::memcpy(f, s.h_frc.data(), sizeof(Vector3D) * n);
+        if (s.mirror_frc_zero) std::memset(f, 0, sizeof(Vector3D) * n);
+        else std::memcpy(f, s.h_frc.data(), sizeof(Vector3D) * n);
     }
     return s.N;
 }

@@ -207,9 +207,11 @@ struct State {
     // first completes the mirror (materialize_mirror).
     int mirror_pending = 0;
     int mirror_n = 0, mirror_na = 0;
+    bool mirror_frc_zero = false;  // the mirror's forces are all zero (not yet written)
+    bool x0_in_pos = false;        // h_x0 is still h_pos (the positions md_initialize_grid got)
     HostVec h_mass;                 // [N+G]
     HostVec h_pos, h_vel, h_frc;    // [(N+G)*3]
-    HostVec h_x0;                   // initial positions (adjoint)
+    HostVec h_x0;                   // initial positions (adjoint), once the mirror's are overwritten
 
     PendingForce pend_force;
     PendingForce force_cfg;   // parameters of the last md_compute_* call
