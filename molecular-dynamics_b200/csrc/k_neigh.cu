@@ -417,9 +417,6 @@ __device__ __forceinline__ int rel_cell(int k, int b) {
 #ifndef TMD_NL_UNROLL
 #define TMD_NL_UNROLL 4
 #endif
-#ifndef TMD_NL_VOTE
-#define TMD_NL_VOTE 0
-#endif
 constexpr int kNlWarps = TMD_NL_WARPS;    // warps (cells) per block
 constexpr int kNlTile = TMD_NL_TILE;      // kept candidates staged per warp before the homes walk them
 constexpr int kNlUnroll = TMD_NL_UNROLL;  // candidates per step of a home's walk
@@ -567,11 +564,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const uint32_t s6 = __float_as_uint(cp.w);  // slot << 6
                 bool in = r2 < a.lo2;
-                const bool near = !in && r2 <= a.hi2;
-#if TMD_NL_VOTE
-                if (__any_sync(0xffffffffu, near))  // rare: a warp-uniform branch around it
-#endif
-                if (near) {
+                if (!in && r2 <= a.hi2) {
                     // near the cutoff: the reference's exact FP64 test
                     const double4 pi = pos[i], pj = pos[s6 >> kCodeBits];
                     in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
