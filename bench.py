@@ -130,6 +130,13 @@ class ClockSampler:
                 if len(parts) >= 9:
                     rows.append(parts)
         os.unlink(self.file.name)
+        if not rows:  # a timed region shorter than the sampling period: one sample right after it
+            try:
+                out = subprocess.run(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-i",
+                                      str(self.index)], capture_output=True, text=True, timeout=10).stdout
+                rows = [[p.strip() for p in line.split(",")] for line in out.splitlines() if line.count(",") >= 8]
+            except (OSError, subprocess.TimeoutExpired):
+                rows = []
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]

@@ -396,6 +396,10 @@ struct ModeGuard {  // the adjoint runs exact ghosts, full lists, its own precis
 };
 
 }  // namespace
+
+// the adjoint's device buffers (checkpoints, adjoints, root lists) go with the grid
+void release_adjoint() { free_adjoint(); }
+
 }  // namespace tmd
 
 using namespace tmd;

@@ -993,6 +993,7 @@ void md_deallocate_grid(void) {
     fold_prof(true);
     phase_reset();
     free_all(s);
+    release_adjoint();
     s.mirror_pending = 0;
     s.alive = false;
     s.N = s.G = 0;

@@ -282,6 +282,7 @@ void run_refresh_pos32(State& s);
 // completes the pending host-mirror copies of the last md_copy_data_from_accelerator (parts:
 // bit 0 locals, bit 1 ghosts)
 void materialize_mirror(State& s, int parts = 3);
+void release_adjoint();  // frees the differentiable form's device buffers (adjoint.cu)
 // list pairs inside the cutoff rc (FP64), the reference's rsq_iters of a force call on the
 // current lists and positions
 long long count_pairs_inside(State& s, double rc);
