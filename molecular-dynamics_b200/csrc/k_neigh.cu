@@ -35,7 +35,7 @@ struct GeoArgs {
     double wlo[3], whi[3], alo[3], ahi[3], len[3];
     double spacing;
     int nx, ny, nz, ncells;
-    double rb_h;
+    double rb_h, inv_rb_h;
 };
 
 GeoArgs geo_args(const Geometry& g) {
@@ -53,6 +53,7 @@ GeoArgs geo_args(const Geometry& g) {
     a.nz = g.nz;
     a.ncells = g.ncells;
     a.rb_h = g.rb_h;
+    a.inv_rb_h = 1.0 / g.rb_h;
     return a;
 }
 
@@ -68,10 +69,13 @@ __device__ __forceinline__ int flat_cell(const double4& p, const GeoArgs& a) {
     return (c >= 0 && c < a.ncells) ? c : a.ncells;
 }
 
+// The rebasing cell is computed here only (the binning's move) and stored, so every kernel sees
+// the same cell; a product with 1 / h instead of a correctly rounded division is enough (a pair
+// within the list cutoff stays within one cell step whatever the rounding at a cell boundary).
 __device__ __forceinline__ int rebase_cell(const double4& p, const GeoArgs& a) {
-    int i = (int)floor((p.x - a.alo[0]) / a.rb_h);
-    int j = (int)floor((p.y - a.alo[1]) / a.rb_h);
-    int k = (int)floor((p.z - a.alo[2]) / a.rb_h);
+    int i = (int)floor((p.x - a.alo[0]) * a.inv_rb_h);
+    int j = (int)floor((p.y - a.alo[1]) * a.inv_rb_h);
+    int k = (int)floor((p.z - a.alo[2]) * a.inv_rb_h);
     return pack3(i, j, k);
 }
 
@@ -176,14 +180,14 @@ __global__ void k_border_emit(double4* __restrict__ pos, double4* __restrict__ v
                               int* __restrict__ bsrc_ref, int* __restrict__ broot_ref, int* __restrict__ bcode,
                               int N, int nblk, int capA, GeoArgs a, int sync_vel) {
     __shared__ int wpre[8][26];
+    __shared__ unsigned char s_rank[26][256];  // a thread's rank among its warp's ghosts of each type
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned m = r < N ? bmask[r] : 0u;
     const unsigned lt = lanemask_lt();
-    int rank[26];
     for (int t = 0; t < 26; ++t) {
         unsigned b = __ballot_sync(0xffffffffu, (m >> t) & 1u);
-        rank[t] = __popc(b & lt);
+        s_rank[t][threadIdx.x] = (unsigned char)__popc(b & lt);
         if (lane == 0) wpre[wid][t] = __popc(b);
     }
     __syncthreads();
@@ -202,11 +206,11 @@ __global__ void k_border_emit(double4* __restrict__ pos, double4* __restrict__ v
     const double mroot = mass[s_root];
     const double4 vroot = vel[s_root];
     const unsigned flags = m >> 26;
-    int gidx[26];
-    for (int t = 0; t < 26; ++t) gidx[t] = ((m >> t) & 1u) ? boff[t * nblk + blockIdx.x] + wpre[wid][t] + rank[t] : -1;
+    // index of this root's ghost of type t (a type whose bit is set)
+    auto gidx = [&](int t) { return boff[t * nblk + blockIdx.x] + wpre[wid][t] + s_rank[t][threadIdx.x]; };
     for (int t = 0; t < 26; ++t) {
         if (!((m >> t) & 1u)) continue;
-        const int g = gidx[t];
+        const int g = gidx(t);
         const int slot = N + g;
         if (slot >= capA) continue;  // the host grows the arrays and redoes the pass
         const int tt = t + 1;
@@ -227,8 +231,8 @@ __global__ void k_border_emit(double4* __restrict__ pos, double4* __restrict__ v
         }
         // source of the last pass: the ghost of the same root without the last axis, or the root
         const int tsrc = tt - e[last] * (last == 0 ? 1 : (last == 1 ? 3 : 9));
-        const int src_ref = tsrc == 0 ? r : N + gidx[tsrc - 1];
-        const int src_slot = tsrc == 0 ? s_root : N + gidx[tsrc - 1];
+        const int src_ref = tsrc == 0 ? r : N + gidx(tsrc - 1);
+        const int src_slot = tsrc == 0 ? s_root : src_ref;  // a ghost's slot is its reference index
         int code = 0;
         for (int d = 0; d < 3; ++d) {
             int ls = (d == last) ? lastsh : 0;
@@ -381,13 +385,20 @@ __global__ void k_ghost_links(LinkArgs l) {
 }
 
 // ---- neighbour lists ---------------------------------------------------------
-// rebasing cell k relative to b, 8 bits per axis with bias 128 (|k - b| < 128 per axis
-// for atoms a few cells apart); differences of two such values carry no borrow while
-// every axis differs by at most 1
-__device__ __forceinline__ int rel_cell(int k, int b) {
-    return (wrap_diff(unpack_axis(k, 0), unpack_axis(b, 0)) + 128) |
-           ((wrap_diff(unpack_axis(k, 1), unpack_axis(b, 1)) + 128) << 8) |
-           ((wrap_diff(unpack_axis(k, 2), unpack_axis(b, 2)) + 128) << 16);
+// rebasing cell k relative to b as dx + 4 dy + 16 dz (signed offsets per axis): for two atoms
+// whose offsets differ by at most 1 on every axis, (c - i) + 21 is exactly the list code
+// (dx+1) | (dy+1) << 2 | (dz+1) << 4 of the pair, each term being 0, 1 or 2 with no carry
+__device__ __forceinline__ int rel_code(int k, int b) {
+    return wrap_diff(unpack_axis(k, 0), unpack_axis(b, 0)) + 4 * wrap_diff(unpack_axis(k, 1), unpack_axis(b, 1)) +
+           16 * wrap_diff(unpack_axis(k, 2), unpack_axis(b, 2));
+}
+constexpr int kCodeBias = 1 + 4 + 16;  // dk + 1 on every axis
+
+// The reference's exact FP64 membership test for a pair near the list cutoff (core/neighborlist.impala:
+// 18-78), which the FP32 prefilter cannot decide (~1 candidate in 150)
+__device__ __forceinline__ bool exact_within(const double4* __restrict__ pos, int i, int j, double cut2) {
+    const double4 pi = pos[i], pj = pos[j];
+    return len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= cut2;
 }
 
 // Warp per cell (core/neighborlist.impala:18-78), one home atom per lane (32 at a time).  The
@@ -434,8 +445,9 @@ __global__ void __launch_bounds__(kNlWarps * 32, TMD_NL_MINB)
 k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
              const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl, DevStatus* st,
              NlArgs a, int cell_blocks, LinkArgs la) {
-    __shared__ float4 s_cpos[kNlWarps][kNlTile];  // kept candidate position (cell-centre relative), w = slot << 6
-    __shared__ int s_crel[kNlWarps][kNlTile];     // its rebasing cell relative to the first home's
+    // kept candidate position (cell-centre relative); w = slot << 6 + its rebasing cell relative to
+    // the first home's (rel_code) + kCodeBias, from which a home's entry is one subtraction
+    __shared__ float4 s_cpos[kNlWarps][kNlTile];
     __shared__ int s_cref[kNlWarps][HM ? kNlTile : 1];
     __shared__ int s_rstart[kNlWarps][54];
     __shared__ int s_rpre[kNlWarps][55];
@@ -494,7 +506,6 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
         const int hn = min(32, h1 - hb);
         const bool home = lane < hn;
         const int i = hb + (home ? lane : 0);
-        const uint32_t i6 = (uint32_t)i << kCodeBits;
         float hx = 1e18f, hy = 1e18f, hz = 1e18f;  // no home: never within the cutoff
         int irel = 0, iref = 0;
         if (home) {
@@ -502,9 +513,12 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
             hx = (float)(p.x - ctr[0]);
             hy = (float)(p.y - ctr[1]);
             hz = (float)(p.z - ctr[2]);
-            irel = rel_cell(rbk[i], rb0);
+            irel = rel_code(rbk[i], rb0);
             if (HM) iref = ref[i];
         }
+        // a candidate's staged w minus irel is the entry slot << 6 | code; it equals i6 only for
+        // the home itself (within the cutoff the two rebasing parts differ by less than 64)
+        const uint32_t i6 = ((uint32_t)i << kCodeBits) + (uint32_t)(irel + kCodeBias);
         // bounding box of the homes, widened by the list cutoff (with the FP32 margin)
         float lo[3] = {home ? hx : INFINITY, home ? hy : INFINITY, home ? hz : INFINITY};
         float hi[3] = {home ? hx : -INFINITY, home ? hy : -INFINITY, home ? hz : -INFINITY};
@@ -524,7 +538,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 const int m = t0 + lane;
                 bool keep = false;
                 float4 cp;
-                int crel = 0, cref = 0;
+                int cref = 0;
                 if (m < M) {
                     int lo_r = 0, hi_r = 53;  // the range of candidate m: the last one starting at or before m
                     while (lo_r < hi_r) {
@@ -538,18 +552,17 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                     const int kb = __ldg(rbk + slot);
                     if (HM) cref = __ldg(ref + slot);  // root reference index (ref for locals)
                     cp = make_float4((float)(p.x - ctr[0]), (float)(p.y - ctr[1]), (float)(p.z - ctr[2]),
-                                     __uint_as_float((uint32_t)slot << kCodeBits));
+                                     __uint_as_float(((uint32_t)slot << kCodeBits) +
+                                                     (uint32_t)(rel_code(kb, rb0) + kCodeBias)));
                     const float ex = fmaxf(fmaxf(lo[0] - cp.x, cp.x - hi[0]), 0.f);
                     const float ey = fmaxf(fmaxf(lo[1] - cp.y, cp.y - hi[1]), 0.f);
                     const float ez = fmaxf(fmaxf(lo[2] - cp.z, cp.z - hi[2]), 0.f);
                     keep = fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= a.hi2;
-                    crel = rel_cell(kb, rb0);
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, keep);
                 if (keep) {
                     const int at = nk + __popc(bal & lt);
                     s_cpos[wid][at] = cp;
-                    s_crel[wid][at] = crel;
                     if (HM) s_cref[wid][at] = cref;
                 }
                 nk += __popc(bal);
@@ -562,30 +575,23 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                 const float4 cp = s_cpos[wid][k];
                 const float dx = hx - cp.x, dy = hy - cp.y, dz = hz - cp.z;
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const uint32_t s6 = __float_as_uint(cp.w);  // slot << 6
+                const uint32_t s6 = __float_as_uint(cp.w);
                 bool in = r2 < a.lo2;
-                if (!in && r2 <= a.hi2) {
-                    // near the cutoff: the reference's exact FP64 test
-                    const double4 pi = pos[i], pj = pos[s6 >> kCodeBits];
-                    in = len2_strict(dsub(pi.x, pj.x), dsub(pi.y, pj.y), dsub(pi.z, pj.z)) <= a.cut2;
-                }
+                // near the cutoff (|dk| <= 1 still holds there): s6 - irel is the entry, its slot the candidate's
+                if (!in && r2 <= a.hi2) in = exact_within(pos, i, (s6 - (uint32_t)irel) >> kCodeBits, a.cut2);
                 // core/neighborlist.impala:34: half lists keep i > j (reference index); HM == 2
                 // compares ghosts by their root so pairs across the periodic boundary are kept once
                 const bool take = in && s6 != i6 && (!HM || s_cref[wid][HM ? k : 0] < iref);
+                // the entry slot << 6 | code: the list cutoff below the rebasing spacing keeps
+                // every |dk| <= 1 within it (checked on the host)
                 if (HM) {
                     // half lists: the append without a branch (measured faster there, while
                     // the full-list walk is faster with the branch)
-                    const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
-                    const uint32_t code = (d + (d >> 6) + (d >> 12)) & kCodeMask;
-                    if (take && cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 | code;
+                    if (take && cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 - (uint32_t)irel;
                     cnt += take ? 1 : 0;
                 } else if (take) {
-                    // dk + 1 per axis in bytes 0-2, packed as x | y << 2 | z << 4 (the three
-                    // shifted copies land in disjoint bits 0-5 without carries); the list cutoff
-                    // below the rebasing spacing keeps every |dk| <= 1 (checked on the host)
-                    const uint32_t d = (uint32_t)(s_crel[wid][k] - irel + 0x010101);
-                    const uint32_t code = (d + (d >> 6) + (d >> 12)) & kCodeMask;
-                    if (cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 | code;
+                    // (a store at every step, without the branch: 147 -> 182 us at 131k atoms)
+                    if (cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 - (uint32_t)irel;
                     ++cnt;
                 }
             }
@@ -594,7 +600,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
         if (home) {
             nbn[i] = cnt;
             // the last quad's padding
-            const uint32_t pad = i6 | kPadCode;
+            const uint32_t pad = ((uint32_t)i << kCodeBits) | kPadCode;
             for (int q = cnt; (q & 3) != 0 && q < a.nbcap; ++q) nbl[nl_index(q, i, a.stride)] = pad;
             maxcnt = max(maxcnt, cnt);
         }

@@ -107,16 +107,8 @@ __device__ __forceinline__ double4 integrate_one(const double4& x, double4& v, d
 
 constexpr int kB64 = 4;  // neighbours per batch (FP64): one list quad
 constexpr int kB32 = 4;  // neighbours per batch (mixed): one list quad
-constexpr int kQ = 8;    // FP64-path neighbours a mixed thread queues before working them off
-// TMD_MX_LEAN: f = sr2 sr6 (48 eps sr6 - 24 eps), one operation fewer per pair.
-// TMD_MX_SLOWPRED: FP64-path pairs queued without a branch (measured with 72 registers:
-// 37.4 -> 35.4 us together with the lean formula; with 64 registers it spilled, 48 us).
-#ifndef TMD_MX_LEAN
-#define TMD_MX_LEAN 1
-#endif
-#ifndef TMD_MX_SLOWPRED
-#define TMD_MX_SLOWPRED 1
-#endif
+// list quads with FP64-path pairs a mixed thread queues (more: the atom is redone in place, rare)
+constexpr int kQQ = 8;
 
 // Ghost images written by the force kernel that integrates (maps from k_ghost_links): each
 // local writes the ghosts that are its images, from its new position, and extra threads
@@ -413,10 +405,12 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
 
 // ---- mixed LJ, branch-free batches (full lists) --------------------------------
 // The pair arithmetic of k_lj_mixed_half, each pair seen from both atoms (no atomics),
-// arranged for instruction-level parallelism: the FP32 fast path of a batch's kB32 pairs runs without branches (the
-// force of a pair outside [close2, rc2_lo) is masked to zero), so the compiler
-// interleaves the pairs' dependent chains; the rare FP64-path pairs of a batch are
-// queued afterwards in list order.  The next batch's list entries are loaded before
+// arranged for instruction-level parallelism: the FP32 fast path of a batch's kB32 pairs (one
+// list quad) runs without branches (the force of a pair outside [close2, rc2_lo) is masked to
+// zero), so the compiler interleaves the pairs' dependent chains; a quad holding FP64-path pairs
+// is queued in shared memory (one store per quad, no branch) and its FP64 pairs are evaluated
+// after the loop, in list order (1 -> 0.99 of the time of a queue of pairs with a per-quad
+// room check, which also spilled in the thermo variants).  The next batch's list entries are loaded before
 // the current batch's gathers, so a batch waits for one memory latency, not two.
 // The atom's FP64 position is re-read where it is needed (FP64 pairs, the epilogue)
 // instead of occupying registers through the loop.
@@ -424,6 +418,36 @@ template <bool THERMO>
 __device__ __forceinline__ void fp64_lj_i(const double4* __restrict__ pos, int i, int j, const LjArgs& a, double& cx,
                                           double& cy, double& cz, double& e, double& w, int& ncnt) {
     fp64_lj<THERMO>(ldg_d4(pos + i), j, pos, a, cx, cy, cz, e, w, ncnt);
+}
+
+// One FP32 pair of k_lj_mixed_bf: the rebasing shift from the entry's code, del, r^2 and, for a
+// fast pair (close2 <= r^2 < rc2_lo), its force added without a branch; returns whether the pair
+// takes the FP64 path (closer than close2, or within the window around the cutoff).
+template <bool THERMO>
+__device__ __forceinline__ bool mixed_pair(uint32_t en, const float4& ri, const float4& rj, const LjArgs& a,
+                                           float& fx, float& fy, float& fz, float& ef, float& wf, int& ncnt) {
+    const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
+    const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
+    const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
+    const float dx = fmaf(a.hx, sx, ri.x - rj.x);
+    const float dy = fmaf(a.hy, sy, ri.y - rj.y);
+    const float dz = fmaf(a.hz, sz, ri.z - rj.z);
+    const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const bool fast = rsq < a.rc2_lo && rsq >= a.close2;
+    float sr2;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
+    const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
+    float f = sr6 * sr2 * fmaf(a.eps48f, sr6, a.eps24nf);
+    f = fast ? f : 0.f;
+    fx = fmaf(dx, f, fx);
+    fy = fmaf(dy, f, fy);
+    fz = fmaf(dz, f, fz);
+    if (THERMO) {
+        ef += fast ? a.eps4f * sr6 * (sr6 - 1.0f) : 0.f;
+        wf = fmaf(f, rsq, wf);
+        ncnt += fast ? 1 : 0;
+    }
+    return !fast && rsq < a.rc2_hi;
 }
 
 template <bool FUSE, bool THERMO, bool INIT = false, bool PUSH = false>
@@ -434,7 +458,9 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
               float4* __restrict__ pos32_n = nullptr, const int* __restrict__ rbk = nullptr,
               PushArgs pa = PushArgs()) {
     __shared__ double scratch[kThreads / 32];
-    __shared__ int s_q[kQ][kThreads];  // each thread's queue of FP64-path neighbours
+    // each thread's queue of list quads holding FP64-path pairs: quad index << kB32 | pair bits;
+    // row kQQ takes the writes past a full queue
+    __shared__ int s_q[kQQ + 1][kThreads];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
@@ -448,7 +474,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
-        int nq = 0;  // deferred FP64 pairs, in s_q[0..nq)[threadIdx.x]
+        int nq = 0;  // list quads with FP64-path pairs, queued in s_q[0..nq)[threadIdx.x]
         // the last quad is padded with the atom itself one rebasing cell away on every axis
         // (rsq = 3h^2 with h above the list cutoff, beyond every window), so a padding entry
         // is neither a fast nor a queued pair and the loop needs no count test
@@ -461,74 +487,44 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
             for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (cur[u] >> kCodeBits));
             // the next quad loads while this one's gathers are in flight
             eq = list_quad(nbl, min(b + 1, nquad - 1), i, a.stride);
-#if TMD_MX_SLOWPRED
-            // room for this quad's FP64 pairs in the queue (rarely short: worked off first)
-            if (__any_sync(__activemask(), nq > kQ - kB32)) {
-                if (nq > kQ - kB32) {
-                    const double4 pi = ldg_d4(pos + i);
-                    for (int q = 0; q < nq; ++q) fp64_lj<THERMO>(pi, s_q[q][threadIdx.x], pos, a, cx, cy, cz, e, w, ncnt);
-                    nq = 0;
-                }
-            }
-#endif
             unsigned slow = 0;
 #pragma unroll
-            for (int u = 0; u < kB32; ++u) {
-                const uint32_t en = cur[u];
-                const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
-                const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
-                const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
-                const float dx = fmaf(a.hx, sx, ri.x - rj[u].x);
-                const float dy = fmaf(a.hy, sy, ri.y - rj[u].y);
-                const float dz = fmaf(a.hz, sz, ri.z - rj[u].z);
-                const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool fast = rsq < a.rc2_lo && rsq >= a.close2;
-#if TMD_MX_SLOWPRED
-                {  // queued without a branch: the slot is written always, counted only for FP64 pairs
-                    const bool sl = !fast && rsq < a.rc2_hi;
-                    s_q[nq][threadIdx.x] = (int)(en >> kCodeBits);
-                    nq += sl ? 1 : 0;
-                }
-#else
-                slow |= (!fast && rsq < a.rc2_hi) ? (1u << u) : 0u;
-#endif
-                float sr2;
-                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
-                const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
-#if TMD_MX_LEAN
-                float f = sr6 * sr2 * fmaf(a.eps48f, sr6, a.eps24nf);
-#else
-                float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
-#endif
-                f = fast ? f : 0.f;
-                fx = fmaf(dx, f, fx);
-                fy = fmaf(dy, f, fy);
-                fz = fmaf(dz, f, fz);
-                if (THERMO) {
-                    ef += fast ? a.eps4f * sr6 * (sr6 - 1.0f) : 0.f;
-                    wf = fmaf(f, rsq, wf);
-                    ncnt += fast ? 1 : 0;
-                }
-            }
-#if !TMD_MX_SLOWPRED
-            while (slow) {  // queued in list order; a full queue is worked off first (rare)
-                const int u = __ffs(slow) - 1;
-                slow &= slow - 1u;
-                const uint32_t en = u == 0 ? cur[0] : (u == 1 ? cur[1] : (u == 2 ? cur[2] : cur[3]));
-                if (nq == kQ) {
-                    const double4 pi = ldg_d4(pos + i);
-                    for (int q = 0; q < kQ; ++q) fp64_lj<THERMO>(pi, s_q[q][threadIdx.x], pos, a, cx, cy, cz, e, w, ncnt);
-                    nq = 0;
-                }
-                s_q[nq++][threadIdx.x] = (int)(en >> kCodeBits);
-            }
-#endif
+            for (int u = 0; u < kB32; ++u)
+                slow |= mixed_pair<THERMO>(cur[u], ri, rj[u], a, fx, fy, fz, ef, wf, ncnt) ? (1u << u) : 0u;
+            // a quad with FP64-path pairs is queued: the slot is written always, counted only then
+            s_q[min(nq, kQQ)][threadIdx.x] = (b << kB32) | (int)slow;
+            nq += slow != 0u ? 1 : 0;
         }
-        // the FP64 pairs of the whole list, worked off together: the warp's lanes run them side
-        // by side instead of one lane at a time inside the loop
-        if (nq > 0) {
+        if (nq > kQQ) {
+            // more quads with FP64-path pairs than the queue holds (dense states): the atom is
+            // redone with its FP64 pairs evaluated in place
+            fx = fy = fz = ef = wf = 0.f;
+            ncnt = 0;
             const double4 pi = ldg_d4(pos + i);
-            for (int q = 0; q < nq; ++q) fp64_lj<THERMO>(pi, s_q[q][threadIdx.x], pos, a, cx, cy, cz, e, w, ncnt);
+            for (int b = 0; b < nquad; ++b) {
+                const uint4 e4 = list_quad(nbl, b, i, a.stride);
+                const uint32_t c4[kB32] = {e4.x, e4.y, e4.z, e4.w};
+                for (int u = 0; u < kB32; ++u) {
+                    const int j = (int)(c4[u] >> kCodeBits);
+                    if (mixed_pair<THERMO>(c4[u], ri, __ldg(pos32 + j), a, fx, fy, fz, ef, wf, ncnt))
+                        fp64_lj<THERMO>(pi, j, pos, a, cx, cy, cz, e, w, ncnt);
+                }
+            }
+        } else if (nq > 0) {
+            // the FP64 pairs of the whole list, worked off together in list order: the warp's
+            // lanes run them side by side instead of one lane at a time inside the loop
+            const double4 pi = ldg_d4(pos + i);
+            for (int q = 0; q < nq; ++q) {
+                const int wq = s_q[q][threadIdx.x];
+                const uint4 e4 = list_quad(nbl, wq >> kB32, i, a.stride);
+                unsigned bits = (unsigned)wq & ((1u << kB32) - 1u);
+                while (bits) {
+                    const int u = __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    const uint32_t en = u == 0 ? e4.x : (u == 1 ? e4.y : (u == 2 ? e4.z : e4.w));
+                    fp64_lj<THERMO>(pi, (int)(en >> kCodeBits), pos, a, cx, cy, cz, e, w, ncnt);
+                }
+            }
         }
         const double Fx = (double)fx + cx, Fy = (double)fy + cy, Fz = (double)fz + cz;
         const float4 F = make_float4((float)Fx, (float)Fy, (float)Fz, 0.f);

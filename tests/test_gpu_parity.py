@@ -209,6 +209,33 @@ def test_mixed_force_error(product, oracle):
         p.close()
 
 
+def test_mixed_force_error_dense(product, oracle):
+    """Mixed form on a compressed lattice (a = 1.3: the 12 nearest neighbours at ~0.92 sigma all
+    take the FP64 path, spread over more list quads than a thread queues, so the kernel redoes
+    such atoms with the FP64 pairs in place): max |dF| / rms(F) <= 1e-5 against the FP64 forces
+    on the same positions."""
+    p = make_sim(product, setup_lib=product, cells=(6, 6, 6), potmin=1.3, nb_capacity=256)
+    try:
+        p.step(0.005, 10)
+        x, _, f64 = tinymd.full_state(product)
+        lists = tinymd.neighbor_lists(product, p.n, capacity=512)
+        most = 0  # list quads holding a pair closer than 1.04 sigma, per atom
+        for i, l in enumerate(lists):
+            d = x[l] - x[i]
+            close = np.nonzero(np.einsum("ij,ij->i", d, d) < 1.04 ** 2)[0]
+            most = max(most, len(set((close // 4).tolist())))
+        assert most > 8, most
+        product.md_set_precision(1)
+        p.force()
+        product.md_final_integration(0.0)
+        _, _, f32 = tinymd.full_state(product)
+        err = rel_err(f32, f64)
+        assert err <= 1e-5, err
+    finally:
+        product.md_set_precision(0)
+        p.close()
+
+
 def test_half_lists_with_ghost_pairs(product, oracle):
     """Corrected half mode: lists equal the oracle's; forces equal the full-list forces."""
     product.md_set_half_mode(1)
