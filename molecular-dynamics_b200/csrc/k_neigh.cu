@@ -440,7 +440,7 @@ struct NlArgs {
     double alo[3], spacing;
 };
 
-template <int HM>
+template <int HM, typename IDX>
 __global__ void __launch_bounds__(kNlWarps * 32, TMD_NL_MINB)
 k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const int* __restrict__ rbk,
              const int* __restrict__ cstart, int* __restrict__ nbn, uint32_t* __restrict__ nbl, DevStatus* st,
@@ -519,6 +519,9 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
         // a candidate's staged w minus irel is the entry slot << 6 | code; it equals i6 only for
         // the home itself (within the cutoff the two rebasing parts differ by less than 64)
         const uint32_t i6 = ((uint32_t)i << kCodeBits) + (uint32_t)(irel + kCodeBias);
+        // nl_index in the list's index type: 32-bit unless the list holds 2^32 entries or more
+        // (the 64-bit index arithmetic made the build 15 % slower)
+        const IDX i4 = HM ? 0 : (IDX)i * 4u, stride4 = HM ? 0 : (IDX)a.stride * 4u;  // (the half lists: nl_index)
         // bounding box of the homes, widened by the list cutoff (with the FP32 margin)
         float lo[3] = {home ? hx : INFINITY, home ? hy : INFINITY, home ? hz : INFINITY};
         float hi[3] = {home ? hx : -INFINITY, home ? hy : -INFINITY, home ? hz : -INFINITY};
@@ -591,7 +594,7 @@ k_build_list(const double4* __restrict__ pos, const int* __restrict__ ref, const
                     cnt += take ? 1 : 0;
                 } else if (take) {
                     // (a store at every step, without the branch: 147 -> 182 us at 131k atoms)
-                    if (cnt < a.nbcap) nbl[nl_index(cnt, i, a.stride)] = s6 - (uint32_t)irel;
+                    if (cnt < a.nbcap) nbl[(IDX)(cnt >> 2) * stride4 + i4 + (IDX)(cnt & 3)] = s6 - (uint32_t)irel;
                     ++cnt;
                 }
             }
@@ -895,6 +898,16 @@ void flush_links(State& s) {
     launched(K_BIN);
 }
 
+template <int HM>
+void launch_build_list(State& s, bool wide, int blocks, const int* ref, const NlArgs& a, int nb, const LinkArgs& la) {
+    if (wide)
+        k_build_list<HM, size_t><<<blocks, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], ref, s.rbk, s.cstart, s.nbn,
+                                                                         s.nbl, s.status_dev, a, nb, la);
+    else
+        k_build_list<HM, uint32_t><<<blocks, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], ref, s.rbk, s.cstart,
+                                                                           s.nbn, s.nbl, s.status_dev, a, nb, la);
+}
+
 int run_build_lists(State& s, bool half, double cutoff) {
     const Geometry& g = s.geo;
     s.lists_cutoff = cutoff;
@@ -929,15 +942,13 @@ int run_build_lists(State& s, bool half, double cutoff) {
         const LinkArgs la = link_args(s);
         const int lb = s.pend_links ? nblocks(s.G, kNlWarps * 32) : 0;
         s.pend_links = false;
+        const bool wide = (size_t)s.nb_cap * s.nb_stride > 0xffffffffull;  // list index beyond 32 bits
         if (half && s.half_ghost)
-            k_build_list<2><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.rref, s.rbk, s.cstart, s.nbn,
-                                                                     s.nbl, s.status_dev, a, nb, la);
+            launch_build_list<2>(s, wide, nb + lb, s.rref, a, nb, la);
         else if (half)
-            k_build_list<1><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                     s.nbn, s.nbl, s.status_dev, a, nb, la);
+            launch_build_list<1>(s, wide, nb + lb, s.ref.b[s.ac], a, nb, la);
         else
-            k_build_list<0><<<nb + lb, kNlWarps * 32, 0, s.stream>>>(s.pos.b[s.pc], s.ref.b[s.ac], s.rbk, s.cstart,
-                                                                     s.nbn, s.nbl, s.status_dev, a, nb, la);
+            launch_build_list<0>(s, wide, nb + lb, s.ref.b[s.ac], a, nb, la);
         launched(K_NLIST);
         prof_end(K_NLIST);
         TMD_CUDA(cudaMemcpyAsync(s.status_host, s.status_dev, sizeof(DevStatus), cudaMemcpyDeviceToHost, s.stream));
