@@ -199,8 +199,6 @@ void prof_reset() {
 // ---------------------------------------------------------------------------
 namespace {
 
-int border_blocks(int N) { return (N + 255) / 256; }
-
 // The per-slot arrays live in one device allocation per capacity: a few dozen allocations of a
 // few MB each took ~11 ms to make and ~9 ms to free on B200, one allocation of their total
 // size ~0.4 ms.  `elems` are the elements per slot, `keep` whether a growth copies the contents.
@@ -251,6 +249,15 @@ void free_all(State& s) {
     if (s.ev_counted) {
         cudaEventDestroy(s.ev_counted);
         s.ev_counted = nullptr;
+    }
+    if (s.ev_scanned) {
+        cudaEventDestroy(s.ev_scanned);
+        s.ev_scanned = nullptr;
+    }
+    if (s.copy_stream) {
+        cudaStreamSynchronize(s.copy_stream);
+        cudaStreamDestroy(s.copy_stream);
+        s.copy_stream = nullptr;
     }
     for (int k = 0; k < kThermoSlots; ++k) {
         if (s.thermo_ev[k]) cudaEventDestroy(s.thermo_ev[k]);
@@ -327,6 +334,8 @@ bool allocate_state(State& s, int N, int nb_cap) {
     s.nb_cap = list_rows(nb_cap > 0 ? nb_cap : 100);
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
     if (!s.ev_counted) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_counted, cudaEventDisableTiming));
+    if (!s.ev_scanned) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_scanned, cudaEventDisableTiming));
+    if (!s.copy_stream) TMD_CUDA(cudaStreamCreateWithFlags(&s.copy_stream, cudaStreamNonBlocking));
     dalloc(&s.thermo_dev, 8);
     dalloc(&s.status_dev, 1);
     if (!s.status_host) TMD_CUDA(cudaMallocHost((void**)&s.status_host, sizeof(DevStatus)));

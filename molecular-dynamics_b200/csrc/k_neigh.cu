@@ -144,10 +144,10 @@ __device__ __forceinline__ unsigned border_mask(const double4& p, const GeoArgs&
 // Pass 1: masks in reference order and per-block per-type counts [26][nblk].  WRAP: the
 // periodic wrap of each local (k_enforce_pbc's) is done here first, one launch fewer.
 template <bool WRAP>
-__global__ void k_border_count(double4* __restrict__ pos, int* __restrict__ img, const int* __restrict__ slot_of_ref,
+__global__ void __launch_bounds__(kBorderThreads) k_border_count(double4* __restrict__ pos, int* __restrict__ img, const int* __restrict__ slot_of_ref,
                                unsigned* __restrict__ bmask, int* __restrict__ bcount, int N, int nblk, GeoArgs a,
                                int* __restrict__ cnt, int nseg, DevStatus* st) {
-    __shared__ int wc[8][26];
+    __shared__ int wc[kBorderThreads / 32][26];
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     // the binning that follows starts from zeroed cell counters and status (no memsets there)
@@ -173,14 +173,14 @@ __global__ void k_border_count(double4* __restrict__ pos, int* __restrict__ img,
 
 // Pass 2 (after an exclusive scan of bcount into boff): writes every ghost at
 // slot N + g, g its reference ghost index, with its source / root links.
-__global__ void k_border_emit(double4* __restrict__ pos, double4* __restrict__ vel, double4* __restrict__ frc,
+__global__ void __launch_bounds__(kBorderThreads) k_border_emit(double4* __restrict__ pos, double4* __restrict__ vel, double4* __restrict__ frc,
                               double* __restrict__ mass, int* __restrict__ ref, int* __restrict__ slot_of_ref,
                               const unsigned* __restrict__ bmask, const int* __restrict__ boff,
                               int* __restrict__ gsrc, int* __restrict__ groot, int* __restrict__ gcode,
                               int* __restrict__ bsrc_ref, int* __restrict__ broot_ref, int* __restrict__ bcode,
                               int N, int nblk, int capA, GeoArgs a, int sync_vel) {
-    __shared__ int wpre[8][26];
-    __shared__ unsigned char s_rank[26][256];  // a thread's rank among its warp's ghosts of each type
+    __shared__ int wpre[kBorderThreads / 32][26];
+    __shared__ unsigned char s_rank[26][kBorderThreads];  // a thread's rank among its warp's ghosts of each type
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const unsigned m = r < N ? bmask[r] : 0u;
@@ -321,27 +321,28 @@ __device__ __forceinline__ void move_slot(int n, int o, const MoveArgs& m, const
     if (m.mixed) m.pos32[n] = rebased32(p, k, a.alo, a.rb_h);
 }
 
+// One thread per new slot: the slot's segment (cell, locals or ghosts) from its old slot's cell,
+// its rank among the segment's members by reference index, then the move.  (A warp per segment
+// left ~45 % of the lanes idle and half the warps on the empty ghost segments of inner cells.)
 __global__ void k_rank_move(const int* __restrict__ cstart, const int* __restrict__ tmp_key,
-                            const int* __restrict__ tmp_src, int nseg, int ncells, MoveArgs m, GeoArgs ga,
+                            const int* __restrict__ tmp_src, int NA, int ncells, MoveArgs m, GeoArgs ga,
                             DevStatus* st) {
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
     // the list build that follows starts from a zeroed status (no memset there)
-    if (blockIdx.x == 0 && threadIdx.x == 0)
-        st->max_nb = 0;
-    if (gw >= nseg) return;
-    const int a = cstart[gw], b = cstart[gw + 1];
-    const bool outside = gw == ncells || gw == 2 * ncells + 1;
-    for (int e = a + lane; e < b; e += 32) {
-        int n = e;
-        if (!outside) {
-            const int key = tmp_key[e];
-            int rank = 0;
-            for (int f = a; f < b; ++f) rank += tmp_key[f] < key;
-            n = a + rank;
-        }
-        move_slot(n, tmp_src[e], m, ga);
+    if (e == 0) st->max_nb = 0;
+    if (e >= NA) return;
+    const int o = tmp_src[e];
+    const int key = tmp_key[e];
+    const int c = m.bin_cell[o];
+    int n = e;  // atoms outside the grid keep their bucket order
+    if (c != ncells) {
+        const int seg = o < m.N ? c : ncells + 1 + c;
+        const int a = cstart[seg], b = cstart[seg + 1];
+        int rank = 0;
+        for (int f = a; f < b; ++f) rank += tmp_key[f] < key;
+        n = a + rank;
     }
+    move_slot(n, o, m, ga);
 }
 
 // Per ghost: its source, root and shift code in slot terms, and its place in the image
@@ -773,7 +774,7 @@ bool grow_atoms(State& s, int need);  // api.cu
 void run_borders(State& s, bool wrap) {
     GeoArgs a = geo_args(s.geo);
     const int N = s.N;
-    const int nblk = nblocks(N, 256);
+    const int nblk = border_blocks(N);
     if (N == 0) {
         s.G = 0;
         return;
@@ -781,10 +782,10 @@ void run_borders(State& s, bool wrap) {
     prof_begin(K_BORDER);
     const int nseg = 2 * (a.ncells + 1);
     if (wrap)
-        k_border_count<true><<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
+        k_border_count<true><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
                                                           s.bcount, N, nblk, a, s.cnt, nseg, s.status_dev);
     else
-        k_border_count<false><<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
+        k_border_count<false><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
                                                            s.bcount, N, nblk, a, s.cnt, nseg, s.status_dev);
     s.bin_zeroed = true;
     launched(K_BORDER);
@@ -796,10 +797,14 @@ void run_borders(State& s, bool wrap) {
     // slots below the capacity, so when the count shows the capacity was short the host
     // grows the arrays (which waits for that emit) and emits again.  The host thus enqueues
     // the next kernels before emit finishes instead of leaving the GPU idle for a round trip.
-    TMD_CUDA(cudaMemcpyAsync(&s.status_host->nghost, boff + n, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-    TMD_CUDA(cudaEventRecord(s.ev_counted, s.stream));
+    // The readback runs on a second stream, so the emit kernel does not queue behind the copy
+    // (a rebuild's ghost phase 40 -> 33 us at 131k atoms).
+    TMD_CUDA(cudaEventRecord(s.ev_scanned, s.stream));
+    TMD_CUDA(cudaStreamWaitEvent(s.copy_stream, s.ev_scanned, 0));
+    TMD_CUDA(cudaMemcpyAsync(&s.status_host->nghost, boff + n, sizeof(int), cudaMemcpyDeviceToHost, s.copy_stream));
+    TMD_CUDA(cudaEventRecord(s.ev_counted, s.copy_stream));
     auto emit = [&]() {
-        k_border_emit<<<nblk, 256, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
+        k_border_emit<<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
                                                   s.ref.b[s.ac], s.slot_of_ref, s.bmask, boff, s.gsrc, s.groot,
                                                   s.gcode, s.bsrc_ref, s.broot_ref, s.bcode, N, nblk, s.capA,
                                                   a, s.dem_fixed);
@@ -852,8 +857,8 @@ void run_distribute(State& s) {
     m.bin_cell = s.bin_cell; m.slot_cell = s.slot_cell;
     m.pos32 = s.pos32.b[np]; m.img_cnt = s.img_cnt; m.img_slot = s.img_slot;
     m.capA = s.capA; m.N = N; m.mixed = s.precision;
-    k_rank_move<<<nblocks((long long)nseg * 32, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, nseg,
-                                                                           a.ncells, m, a, s.status_dev);
+    k_rank_move<<<nblocks(NA, 256), 256, 0, s.stream>>>(s.cstart, s.tmp_key, s.tmp_src, NA, a.ncells, m, a,
+                                                         s.status_dev);
     launched(K_BIN);
     s.build_zeroed = true;
     s.pc = np;

@@ -111,6 +111,11 @@ constexpr int kImgW = kImg1 + kImg2;
 
 constexpr int kThermoSlots = 8;  // asynchronous thermo reads in flight at most
 
+// threads per block of the ghost count and emit kernels: the ghost offsets are scanned over
+// 26 types x blocks, so larger blocks make that scan shorter
+constexpr int kBorderThreads = 1024;
+inline int border_blocks(int N) { return (N + kBorderThreads - 1) / kBorderThreads; }
+
 struct PendingForce {
     bool valid = false;
     bool dem = false;
@@ -194,6 +199,8 @@ struct State {
     DevStatus* status_dev = nullptr;
     DevStatus* status_host = nullptr;  // pinned
     cudaEvent_t ev_counted = nullptr;  // the ghost count's readback (run_borders)
+    cudaEvent_t ev_scanned = nullptr;  // the ghost offsets scanned (the readback waits on it)
+    cudaStream_t copy_stream = nullptr;  // the ghost count's readback, beside the emit kernel
     int scan_attr_device = -1;         // device whose k_scan_single shared-memory attribute is set
     double* thermo_host = nullptr;     // pinned [kThermoSlots][4]: asynchronous thermo reads
     cudaEvent_t thermo_ev[8] = {};     // one per slot: its copy has landed
