@@ -410,10 +410,10 @@ def workloads(lib, tm, flush, peak):
                                    "frac": achieved / peak, "launch_ms": launch_ms, "bytes_per_atom": b32,
                                    "force_bytes_per_atom": fb, "integrate_ghost_bytes_per_atom": sb,
                                    "mean_list_length": mean_nb,
-                                   # ncu at this size: 262 MB of DRAM traffic per launch in 120 us (2.2 TB/s,
-                                   # 0.33 of the measured peak); the neighbour gathers are served by L2
-                                   "traffic": 262.1e6, "traffic_source": "profiles/lj_mixed_full_524k_dram.md",
-                                   "limiter": "instruction issue and latency (73 M warp instructions per launch)"}
+                                   # ncu at this size: 263 MB of DRAM traffic per launch in 116 us (2.3 TB/s,
+                                   # 0.35 of the measured peak); the neighbour gathers are served by L2
+                                   "traffic": 263.2e6, "traffic_source": "profiles/lj_mixed_full_524k_dram.md",
+                                   "limiter": "instruction issue and latency (71 M warp instructions per launch)"}
     out["lj_half_fcc_64x64x64_524288_atoms_full_list"] = row
     # DEM at 48^3: the FCC diagonal split and the reference's granular gas, with the
     # reference closure (zero force) and the contact-fixed model (R = 0.6)
@@ -588,8 +588,8 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "kernel": "force_lj (mixed, full list)",
                      # what the ncu capture of this kernel shows limits it (profiles/lj_mixed_full_131k_ncu.md)
-                     "limiter": "instruction issue and latency, not HBM: ncu issue active 61 %, DRAM 20 % of peak, "
-                                "gathers served by L1 (75 % hit) and L2",
+                     "limiter": "instruction issue and latency, not HBM: ncu issue active 59 %, DRAM 21 % of peak, "
+                                "gathers served by L1 (74 % hit) and L2",
                      "traffic_frac": (traffic / (force_ms * 1e-3) / 1e9 / peak) if traffic else None,
                      "bytes_per_atom": bytes_per_atom, "force_bytes_per_atom": force_bytes,
                      "integrate_ghost_bytes_per_atom": step_bytes, "mean_list_length": mean_nb,
