@@ -254,6 +254,12 @@ void free_all(State& s) {
         cudaEventDestroy(s.ev_scanned);
         s.ev_scanned = nullptr;
     }
+    if (s.ev_status) {
+        cudaEventSynchronize(s.ev_status);
+        cudaEventDestroy(s.ev_status);
+        s.ev_status = nullptr;
+    }
+    s.status_pending = false;
     if (s.copy_stream) {
         cudaStreamSynchronize(s.copy_stream);
         cudaStreamDestroy(s.copy_stream);
@@ -335,6 +341,7 @@ bool allocate_state(State& s, int N, int nb_cap) {
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
     if (!s.ev_counted) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_counted, cudaEventDisableTiming));
     if (!s.ev_scanned) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_scanned, cudaEventDisableTiming));
+    if (!s.ev_status) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_status, cudaEventDisableTiming));
     if (!s.copy_stream) TMD_CUDA(cudaStreamCreateWithFlags(&s.copy_stream, cudaStreamNonBlocking));
     dalloc(&s.thermo_dev, 8);
     dalloc(&s.status_dev, 1);
@@ -363,6 +370,7 @@ bool require_alive(const char* what) {
 // deferred work
 // ---------------------------------------------------------------------------
 void launch_force(State& s, const PendingForce& p, bool fuse_final, double dt) {
+    resolve_lists(s);
     s.last_force_half = p.half ? 1 : 0;
     if (p.dem) run_force_dem(s, p);
     else run_force_lj(s, p, fuse_final, dt);
@@ -421,7 +429,12 @@ void flush_pbc(State& s) {
     run_enforce_pbc(s);
 }
 
-void flush_all(State& s) {
+// resolve: complete a deferred list build even when nothing else is pending (calls that read
+// the host-side state); md_compute_* only queue a force and skip that
+void flush_all(State& s, bool resolve = true) {
+    if (resolve || s.pend_links || s.pend_final || s.pend_ghost || s.pend_init || s.pend_kick ||
+        s.pend_force.valid || s.pend_pbc)
+        resolve_lists(s);
     flush_links(s);
     flush_final(s);
     flush_ghost(s);
@@ -434,6 +447,7 @@ void flush_all(State& s) {
 // everything but the carried-over ghosts: for calls that touch only the locals, so that a
 // following md_borders, which writes every ghost anew, can drop the carry
 void flush_locals(State& s) {
+    resolve_lists(s);
     flush_links(s);
     flush_final(s);
     flush_init(s);
@@ -804,7 +818,7 @@ void md_assemble_neighborlists(bool half, double cutoff) {
     flush_all(s);
     if (hold) s.pend_links = true;
     phase_mark(PH_NEIGH);
-    run_build_lists(s, half, cutoff);
+    run_build_lists(s, half, cutoff, true);
 }
 
 void md_initial_integration(double dt) {
@@ -831,6 +845,7 @@ void md_initial_integration(double dt) {
 void md_synchronize_ghost_layer(void) {
     State& s = g_state;
     if (!require_alive("md_synchronize_ghost_layer")) return;
+    resolve_lists(s);
     flush_links(s);
     flush_pbc(s);  // ghosts are refreshed from the wrapped locals
     flush_final(s);
@@ -858,7 +873,7 @@ void md_synchronize_ghost_layer(void) {
 void md_compute_lennard_jones(bool half, double rc, double eps, double sigma) {
     State& s = g_state;
     if (!require_alive("md_compute_lennard_jones")) return;
-    flush_all(s);
+    flush_all(s, false);
     PendingForce p;
     p.valid = true;
     p.dem = false;
@@ -876,7 +891,7 @@ void md_compute_lennard_jones(bool half, double rc, double eps, double sigma) {
 void md_compute_dem(bool half, double rc, double damping_n, double damping_t, double stiffness, double friction) {
     State& s = g_state;
     if (!require_alive("md_compute_dem")) return;
-    flush_all(s);
+    flush_all(s, false);
     PendingForce p;
     p.valid = true;
     p.dem = true;

@@ -913,9 +913,38 @@ void launch_build_list(State& s, bool wide, int blocks, const int* ref, const Nl
                                                                            s.nbn, s.nbl, s.status_dev, a, nb, la);
 }
 
-int run_build_lists(State& s, bool half, double cutoff) {
+// A list build's status, read back: the locals outside the grid get empty lists, the two-phase
+// chain and image-map state of the links; 0 when the lists stand, 1 when the capacity was short
+// (grown: the build is to be redone).
+static int finish_build(State& s, bool half) {
+    const Geometry& g = s.geo;
+    if (s.status_host->out_local > 0) {
+        int first_out = 0;
+        // locals outside the grid sit at [cstart[ncells], N): empty lists
+        TMD_CUDA(cudaMemcpyAsync(&first_out, s.cstart + g.ncells, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
+        TMD_CUDA(cudaStreamSynchronize(s.stream));
+        k_clear_lists<<<nblocks(s.N - first_out, 256), 256, 0, s.stream>>>(s.nbn, first_out, s.N);
+        launched(K_NLIST);
+        set_error(5, "locals outside the cell grid at binning (they have no neighbours)");
+    }
+    s.nchain = s.status_host->nchain;
+    s.img_ok = (s.status_host->img_over1 == 0 ? 1 : 0) | (s.status_host->img_over2 == 0 ? 2 : 0);
+    const int mx = s.status_host->max_nb;
+    if (mx <= s.nb_cap) {
+        s.lists_valid = 1;
+        s.lists_half = half;
+        return 0;
+    }
+    // core/neighborlist.impala:74-76: grow to twice the overflow and redo
+    std::printf("0> reallocate_neighborlist_capacity(): %d\n", mx * 2);
+    grow_lists(s, mx * 2);
+    return 1;
+}
+
+int run_build_lists(State& s, bool half, double cutoff, bool defer) {
     const Geometry& g = s.geo;
     s.lists_cutoff = cutoff;
+    s.status_pending = false;
     if (s.N == 0) {
         s.lists_valid = 1;
         s.lists_half = half;
@@ -957,30 +986,30 @@ int run_build_lists(State& s, bool half, double cutoff) {
         launched(K_NLIST);
         prof_end(K_NLIST);
         TMD_CUDA(cudaMemcpyAsync(s.status_host, s.status_dev, sizeof(DevStatus), cudaMemcpyDeviceToHost, s.stream));
-        TMD_CUDA(cudaStreamSynchronize(s.stream));
-        if (s.status_host->out_local > 0) {
-            int first_out = 0;
-            // locals outside the grid sit at [cstart[ncells], N): empty lists
-            TMD_CUDA(cudaMemcpyAsync(&first_out, s.cstart + g.ncells, sizeof(int), cudaMemcpyDeviceToHost, s.stream));
-            TMD_CUDA(cudaStreamSynchronize(s.stream));
-            k_clear_lists<<<nblocks(s.N - first_out, 256), 256, 0, s.stream>>>(s.nbn, first_out, s.N);
-            launched(K_NLIST);
-            set_error(5, "locals outside the cell grid at binning (they have no neighbours)");
-        }
-        s.nchain = s.status_host->nchain;
-        s.img_ok = (s.status_host->img_over1 == 0 ? 1 : 0) | (s.status_host->img_over2 == 0 ? 2 : 0);
-        const int mx = s.status_host->max_nb;
-        if (mx <= s.nb_cap) {
-            s.lists_valid = 1;
-            s.lists_half = half;
+        if (defer && attempt == 0) {
+            // the host goes on; the next force kernel is launched on these lists at once and
+            // resolve_lists reads the status while it runs
+            TMD_CUDA(cudaEventRecord(s.ev_status, s.stream));
+            s.status_pending = true;
+            s.status_half = half;
+            s.lists_valid = 0;
             return 0;
         }
-        // core/neighborlist.impala:74-76: grow to twice the overflow and redo
-        std::printf("0> reallocate_neighborlist_capacity(): %d\n", mx * 2);
-        grow_lists(s, mx * 2);
+        TMD_CUDA(cudaStreamSynchronize(s.stream));
+        if (finish_build(s, half) == 0) return 0;
     }
     set_error(2, "neighbour list capacity did not converge");
     return -1;
+}
+
+int resolve_lists(State& s) {
+    if (!s.status_pending) return 0;
+    s.status_pending = false;
+    TMD_CUDA(cudaEventSynchronize(s.ev_status));
+    const bool outside = s.status_host->out_local > 0;
+    if (finish_build(s, s.status_half) == 0) return outside ? 1 : 0;
+    // the capacity was short: the build again, on the grown lists
+    return run_build_lists(s, s.status_half, s.lists_cutoff) == 0 ? 1 : -1;
 }
 
 }  // namespace tmd

@@ -121,6 +121,7 @@ struct PushArgs {
     const int* gcode = nullptr;
     const int* rbk = nullptr;
     int nchain = 0;              // two-phase mode only
+    const int* nchain_dev = nullptr;  // the count on the device (nchain is then a bound)
     int base = 0;                // shift field of the code: 0 last pass, 8 total
     int planes = 0;              // image planes of the mode
     int plane = 0;               // plane stride (slot capacity)
@@ -187,6 +188,7 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
           const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot,
           double* __restrict__ part, LjArgs a, double4* __restrict__ pos_n = nullptr, PushArgs pa = PushArgs()) {
     __shared__ double scratch[kThreads / 32];
+    if (INIT && lists_failed(a)) return;  // the whole grid returns: nothing written
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_share(pos, (size_t)a.NA * sizeof(double4));
@@ -258,7 +260,7 @@ k_lj_fp64(const double4* __restrict__ pos, double4* __restrict__ frc, double4* _
                 vel[i] = v;
             }
         }
-    } else if (PUSH && i < a.N + pa.nchain) {
+    } else if (PUSH && i < a.N + (pa.nchain_dev ? *pa.nchain_dev : pa.nchain)) {
         push_chain<false>(i - a.N, pos, a.N, pa, pos_n, nullptr, a.alo, a.rb_h);
     }
     if (THERMO) {
@@ -468,6 +470,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
     // each thread's queue of list quads holding FP64-path pairs: quad index << kB32 | pair bits;
     // row kQQ takes the writes past a full queue
     __shared__ int s_q[kQQ + 1][kThreads];
+    if (INIT && lists_failed(a)) return;  // the whole grid returns: nothing written
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
@@ -559,7 +562,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
             w += (double)wf;
             cnt = (double)ncnt;
         }
-    } else if (PUSH && i < a.N + pa.nchain) {
+    } else if (PUSH && i < a.N + (pa.nchain_dev ? *pa.nchain_dev : pa.nchain)) {
         push_chain<true>(i - a.N, pos, a.N, pa, pos_n, pos32_n, a.alo, a.rb_h);
     }
     if (THERMO) {
@@ -1087,7 +1090,10 @@ bool force_init_fusable(const State& s, const PendingForce& p) {
 
 void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double dt_init) {
     const int N = s.N;
-    if (N == 0) return;  // no ghosts either
+    if (N == 0) {
+        resolve_lists(s);
+        return;  // no ghosts either
+    }
     LjArgs a = lj_args(s, p, dt_final);
     if (s.precision == 1) {
         check_mixed_cutoff(s, a);
@@ -1098,9 +1104,14 @@ void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double 
     a.hz = (float)(-s.geo.rb_h / 16.0);
     a.dt_i = dt_init;
     a.h_i = 0.5 * dt_init;
+    // Right after a list build whose status is still in flight the kernel runs on the lists at
+    // once: it returns without writing if that build failed, the two-phase chain count comes
+    // from the device, and the image maps are taken as complete (checked below).
+    const bool spec = s.status_pending;
+    if (spec) a.spec = s.status_dev;
     // the ghosts of the current mode are written too when the image maps are complete
     const int gm = s.ghost_exact ? 2 : 1;
-    const bool push = s.G > 0 && ((s.img_ok >> (gm - 1)) & 1);
+    const bool push = s.G > 0 && (spec || ((s.img_ok >> (gm - 1)) & 1));
     PushArgs pa;
     if (push) {
         pa.slot = s.img_slot + (gm == 2 ? (size_t)kImg1 * s.capA : 0);
@@ -1111,7 +1122,8 @@ void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double 
         pa.gsrc = s.gsrc;
         pa.gcode = s.gcode;
         pa.rbk = s.rbk;
-        pa.nchain = gm == 1 ? s.nchain : 0;
+        pa.nchain = gm == 1 ? (spec ? s.G : s.nchain) : 0;
+        if (spec && gm == 1) pa.nchain_dev = &s.status_dev->nchain;
         pa.base = gm == 1 ? 0 : 8;
         for (int d = 0; d < 3; ++d) pa.len[d] = s.geo.len[d];
     }
@@ -1128,8 +1140,18 @@ void run_force_lj_init(State& s, const PendingForce& p, double dt_final, double 
     }
     launched(K_FORCE_LJ);
     prof_end(K_FORCE_LJ);
+    bool pushed = push;
+    if (spec) {
+        const int r = resolve_lists(s);
+        if (r != 0) {
+            // the kernel returned without writing: the lists are rebuilt (or the error latched)
+            if (r > 0) run_force_lj_init(s, p, dt_final, dt_init);
+            return;
+        }
+        pushed = push && ((s.img_ok >> (gm - 1)) & 1);  // incomplete maps: the ghosts are refreshed
+    }
     s.pc = 1 - s.pc;  // the locals of the other buffer are current; its ghosts follow
-    s.ghosts_pushed = (push || s.G == 0) ? gm : 0;
+    s.ghosts_pushed = (pushed || s.G == 0) ? gm : 0;
     s.integration_iters = N;
     if (thermo) {
         k_reduce_partials<<<1, 256, 0, s.stream>>>(s.red_part, s.thermo_dev, nb, 0, kThermoQ);

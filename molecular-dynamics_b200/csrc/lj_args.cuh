@@ -14,7 +14,14 @@ struct LjArgs {
     // mixed form
     float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f, eps24nf;
     float hx, hy, hz;  // shift decode scales (see the kernels)
+    // a launch on lists whose build status is still in flight: the kernel returns without
+    // writing when that build overflowed the capacity or left locals outside the grid
+    const DevStatus* spec = nullptr;
 };
+
+__device__ __forceinline__ bool lists_failed(const LjArgs& a) {
+    return a.spec != nullptr && (a.spec->max_nb > a.nbcap || a.spec->out_local > 0);
+}
 
 // utils/utilities.impala:27-36 (recursive squaring) for integer powers
 inline double ipow(double x, int n) {

@@ -192,6 +192,11 @@ struct State {
     int* nbn = nullptr;
     uint32_t* nbl = nullptr;
     double lists_cutoff = 0.0;
+    // A list build's status (overflow, locals outside the grid, two-phase chain, image maps)
+    // comes back while the next force kernel already runs: resolve_lists reads it.
+    bool status_pending = false;
+    bool status_half = false;  // the pending build's list mode (a redo after a capacity growth)
+    cudaEvent_t ev_status = nullptr;
     // scan scratch, reductions, status
     int* scan_part = nullptr;  int scan_part_cap = 0;
     double* red_part = nullptr; int red_part_cap = 0;
@@ -277,7 +282,11 @@ void run_enforce_pbc(State& s);
 void flush_links(State& s);                      // the deferred ghost links of a binning, if pending
 void run_borders(State& s, bool wrap = false);   // ghost generation, reference order (wrap: the periodic wrap first)
 void run_distribute(State& s);                    // binning + reorder
-int run_build_lists(State& s, bool half, double cutoff);  // returns 0 or error
+// defer: the status readback is left in flight (resolve_lists completes it)
+int run_build_lists(State& s, bool half, double cutoff, bool defer = false);  // returns 0 or error
+// completes a deferred list build: 0 when the lists stand, 1 when they were rebuilt (a force
+// kernel launched on them speculatively returned without writing), -1 on an error
+int resolve_lists(State& s);
 void run_force_lj(State& s, const PendingForce& p, bool fuse_final, double dt);
 void run_force_dem(State& s, const PendingForce& p);
 // kick_dt >= 0: the previous step's final kick of kick_dt is applied first (held back by

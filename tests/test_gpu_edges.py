@@ -43,6 +43,14 @@ def test_list_capacity_growth(product, oracle):
     run_both(product, oracle, 40, cells=(6, 6, 6), nb_capacity=8)
 
 
+def test_list_capacity_growth_at_a_rebuild(product, oracle):
+    """List capacity 80: the lattice's 78 neighbours fit, the liquid's longest list at the first
+    rebuild (step 20) does not.  The force kernel that the next step launches on those lists
+    before their status is read returns without writing; the lists grow, are built again and the
+    kernel runs again: 40 steps stay bit-identical."""
+    run_both(product, oracle, 40, cells=(6, 6, 6), nb_capacity=80)
+
+
 def test_ghost_capacity_growth(product, oracle):
     """2x2x2 unit cells: 32 atoms and 633 ghosts, far above the initial slot capacity; 40 steps
     bit-identical."""
