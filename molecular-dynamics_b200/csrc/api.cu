@@ -609,9 +609,17 @@ using namespace tmd;
 
 extern "C" {
 
-int md_last_error(void) { return g_state.last_error; }
-const char* md_last_error_string(void) { return g_state.last_error_msg.c_str(); }
+// a list build whose status is still in flight may latch an error (locals outside the grid)
+int md_last_error(void) {
+    if (g_state.alive) resolve_lists(g_state);
+    return g_state.last_error;
+}
+const char* md_last_error_string(void) {
+    if (g_state.alive) resolve_lists(g_state);
+    return g_state.last_error_msg.c_str();
+}
 void md_clear_error(void) {
+    if (g_state.alive) resolve_lists(g_state);
     g_state.last_error = 0;
     g_state.last_error_msg.clear();
 }
