@@ -280,10 +280,10 @@ __global__ void k_bin_scatter(const int* __restrict__ ref, const int* __restrict
     tmp_src[p] = s;
 }
 
-// One warp per segment: rank the members by reference index (keys are unique) and move
-// each one from its old slot to its new one (cstart[segment] + rank).  The two outside-
-// the-grid buckets keep arrival order: their members have no neighbours and are nobody's
-// neighbour, so their order is not observable.
+// The members of a segment (a cell's locals or its ghosts) ranked by reference index (keys are
+// unique), each moved from its old slot to its new one (cstart[segment] + rank).  The two
+// outside-the-grid buckets keep arrival order: their members have no neighbours and are
+// nobody's neighbour, so their order is not observable.
 struct MoveArgs {
     const double4* pos_o; double4* pos_n;
     const double4* vel_o; double4* vel_n;
