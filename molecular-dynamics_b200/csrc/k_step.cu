@@ -309,18 +309,63 @@ __device__ __forceinline__ void fp64_lj(const double4& pi, int j, const double4*
 // del = (r_i - r_j) - dk*rb_h, with dk in {-1,0,1}^3 decoded from the list
 // entry's low bits (exact float construction, 3 operations per axis) and the
 // product exact, so del carries one rounding more than r_i - r_j.  Pairs
-// closer than sigma (large forces, ~0.2 per atom in a dense LJ liquid) and
-// pairs within 1e-3 of the cutoff take the FP64 path, so list membership and
-// the cutoff test stay exactly the FP64 decisions.
+// closer than 1.04 sigma (large forces, ~1 per atom in a dense LJ liquid) and
+// pairs within 2e-5 (relative) of the squared cutoff take the FP64 path, so list
+// membership and the cutoff test stay exactly the FP64 decisions (lj_args).
 //
 // Half lists: each pair once, the reaction added atomically to j (or to the root of
 // a ghost j); forces must be zeroed before the launch.
+
+// del and r^2 of one mixed-form pair from its list entry (the rebasing shift decoded from the
+// entry's code) and the fast-window test, shared by the kernels so that they decide alike
+__device__ __forceinline__ float mixed_del(uint32_t en, const float4& ri, const float4& rj, const LjArgs& a,
+                                           float& dx, float& dy, float& dz) {
+    const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
+    const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
+    const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
+    dx = fmaf(a.hx, sx, ri.x - rj.x);
+    dy = fmaf(a.hy, sy, ri.y - rj.y);
+    dz = fmaf(a.hz, sz, ri.z - rj.z);
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+__device__ __forceinline__ bool mixed_fast(float rsq, const LjArgs& a) { return rsq < a.rc2_lo && rsq >= a.close2; }
+
+// FP64 evaluation of one half-list pair of the mixed form, its reaction added to j's root
+template <bool THERMO>
+__device__ __forceinline__ void fp64_lj_half(const double4& pi, int j, const double4* __restrict__ pos,
+                                             float4* __restrict__ frc32, const int* __restrict__ groot,
+                                             const LjArgs& a, double& cx, double& cy, double& cz, double& e,
+                                             double& w, int& ncnt) {
+    const double4 pj = ldg_d4(pos + j);
+    const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
+    const double r2 = len2_strict(ex, ey, ez);
+    if (r2 < a.rc2) {
+        const double sr2 = recip64(r2);
+        const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
+        const double f = 48.0 * sr6 * (sr6 - 0.5) * sr2 * a.eps;
+        cx += ex * f;
+        cy += ey * f;
+        cz += ez * f;
+        add_force32(frc32 + reaction_slot(j, a.N, groot), (float)(-ex * f), (float)(-ey * f), (float)(-ez * f));
+        if (THERMO) {
+            e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
+            w += f * r2;
+            ncnt++;
+        }
+    }
+}
+
+// The full-list kernel's arrangement over half lists: the FP32 pair force of a quad without
+// branches, the reaction added (one vector atomic) for the pairs in the fast window, and the quads
+// holding FP64-path pairs queued and worked off after the loop (49.1 -> 42.5 us at 131k atoms
+// against one branch per pair with the FP64 path inline).
 template <bool THERMO>
 __global__ void __launch_bounds__(kThreads, TMD_MINB)
 k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ pos, float4* __restrict__ frc32,
                 const int* __restrict__ nbn, const uint32_t* __restrict__ nbl, const int* __restrict__ groot,
                 double* __restrict__ part, LjArgs a) {
     __shared__ double scratch[kThreads / 32];
+    __shared__ int s_q[kQQ + 1][kThreads];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int n = i < a.N ? min(nbn[i], a.nbcap) : 0;
     prefetch_share(pos32, (size_t)a.NA * sizeof(float4));
@@ -328,65 +373,73 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
     double e = 0.0, w = 0.0, cnt = 0.0;
     if (i < a.N) {
         const float4 ri = pos32[i];
-        const double4 pi = pos[i];
         float fx = 0.f, fy = 0.f, fz = 0.f, ef = 0.f, wf = 0.f;
         double cx = 0.0, cy = 0.0, cz = 0.0;
         int ncnt = 0;
-        const int nq = (n + 3) >> 2;
-        for (int b = 0; b < nq; ++b) {
-            const int k0 = 4 * b;
-            const uint4 eq = list_quad(nbl, b, i, a.stride);  // entries past n are padding (skipped)
-            const uint32_t ent[kB32] = {eq.x, eq.y, eq.z, eq.w};
+        int nq = 0;
+        // the last quad's padding (the atom itself one rebasing cell away) is in no window
+        const int nquad = (n + 3) >> 2;
+        uint4 eq = n > 0 ? list_quad(nbl, 0, i, a.stride) : make_uint4(0u, 0u, 0u, 0u);
+        for (int b = 0; b < nquad; ++b) {
+            const uint32_t cur[kB32] = {eq.x, eq.y, eq.z, eq.w};
             float4 rj[kB32];
 #pragma unroll
-            for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (ent[u] >> kCodeBits));
+            for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (cur[u] >> kCodeBits));
+            eq = list_quad(nbl, min(b + 1, nquad - 1), i, a.stride);
+            unsigned slow = 0;
 #pragma unroll
             for (int u = 0; u < kB32; ++u) {
-                if (k0 + u >= n) continue;
-                const uint32_t en = ent[u];
-                const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
-                const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
-                const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
-                const float dx = fmaf(a.hx, sx, ri.x - rj[u].x);
-                const float dy = fmaf(a.hy, sy, ri.y - rj[u].y);
-                const float dz = fmaf(a.hz, sz, ri.z - rj[u].z);
-                const float rsq = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                if (!(rsq < a.rc2_hi)) continue;
-                const int j = (int)(en >> kCodeBits);
-                const int t = reaction_slot(j, a.N, groot);
-                if (rsq < a.rc2_lo && rsq >= a.close2) {
-                    float sr2;  // hardware reciprocal (~1 ulp); the error budget is set by del, not by 1/r^2
-                    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
-                    const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
-                    const float f = a.eps48f * sr6 * (sr6 - 0.5f) * sr2;
-                    const float px = dx * f, py = dy * f, pz = dz * f;
-                    fx += px;
-                    fy += py;
-                    fz += pz;
-                    add_force32(frc32 + t, -px, -py, -pz);
-                    if (THERMO) {
-                        ef += a.eps4f * sr6 * (sr6 - 1.0f);
-                        wf += f * rsq;
-                        ncnt++;
+                float dx, dy, dz;
+                const float rsq = mixed_del(cur[u], ri, rj[u], a, dx, dy, dz);
+                const bool fast = mixed_fast(rsq, a);
+                float sr2;
+                asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
+                const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
+                float f = sr6 * sr2 * fmaf(a.eps48f, sr6, a.eps24nf);
+                f = fast ? f : 0.f;
+                const float px = dx * f, py = dy * f, pz = dz * f;
+                fx += px;
+                fy += py;
+                fz += pz;
+                if (fast) add_force32(frc32 + reaction_slot((int)(cur[u] >> kCodeBits), a.N, groot), -px, -py, -pz);
+                if (THERMO) {
+                    ef += fast ? a.eps4f * sr6 * (sr6 - 1.0f) : 0.f;
+                    wf = fmaf(f, rsq, wf);
+                    ncnt += fast ? 1 : 0;
+                }
+                slow |= (!fast && rsq < a.rc2_hi) ? (1u << u) : 0u;
+            }
+            s_q[min(nq, kQQ)][threadIdx.x] = (b << kB32) | (int)slow;
+            nq += slow != 0u ? 1 : 0;
+        }
+        if (nq > 0) {
+            const double4 pi = ldg_d4(pos + i);
+            if (nq > kQQ) {
+                // more queued quads than the queue holds: every quad is tested again (the same
+                // arithmetic, so the same pairs) and its FP64 pairs evaluated in place
+                for (int b = 0; b < nquad; ++b) {
+                    const uint4 e4 = list_quad(nbl, b, i, a.stride);
+                    const uint32_t c4[kB32] = {e4.x, e4.y, e4.z, e4.w};
+                    for (int u = 0; u < kB32; ++u) {
+                        float dx, dy, dz;
+                        const float rsq = mixed_del(c4[u], ri, __ldg(pos32 + (c4[u] >> kCodeBits)), a, dx, dy, dz);
+                        if (!mixed_fast(rsq, a) && rsq < a.rc2_hi)
+                            fp64_lj_half<THERMO>(pi, (int)(c4[u] >> kCodeBits), pos, frc32, groot, a, cx, cy, cz, e, w,
+                                                 ncnt);
                     }
-                } else {
-                    // FP64 path: exact cutoff decision and close-contact accuracy
-                    const double4 pj = ldg_d4(pos + j);
-                    const double ex = dsub(pi.x, pj.x), ey = dsub(pi.y, pj.y), ez = dsub(pi.z, pj.z);
-                    const double r2 = len2_strict(ex, ey, ez);
-                    if (r2 < a.rc2) {
-                        const double sr2 = recip64(r2);
-                        const double sr6 = sr2 * sr2 * sr2 * a.sigma6;
-                        const double f = 48.0 * sr6 * (sr6 - 0.5) * sr2 * a.eps;
-                        cx += ex * f;
-                        cy += ey * f;
-                        cz += ez * f;
-                        add_force32(frc32 + t, (float)(-ex * f), (float)(-ey * f), (float)(-ez * f));
-                        if (THERMO) {
-                            e += 4.0 * a.eps * sr6 * (sr6 - 1.0);
-                            w += f * r2;
-                            ncnt++;
-                        }
+                }
+            } else {
+                uint4 nx4 = list_quad(nbl, s_q[0][threadIdx.x] >> kB32, i, a.stride);
+                for (int q = 0; q < nq; ++q) {
+                    const int wq = s_q[q][threadIdx.x];
+                    const uint4 e4 = nx4;
+                    if (q + 1 < nq) nx4 = list_quad(nbl, s_q[q + 1][threadIdx.x] >> kB32, i, a.stride);
+                    unsigned bits = (unsigned)wq & ((1u << kB32) - 1u);
+                    while (bits) {
+                        const int u = __ffs(bits) - 1;
+                        bits &= bits - 1u;
+                        const uint32_t en = u == 0 ? e4.x : (u == 1 ? e4.y : (u == 2 ? e4.z : e4.w));
+                        fp64_lj_half<THERMO>(pi, (int)(en >> kCodeBits), pos, frc32, groot, a, cx, cy, cz, e, w, ncnt);
                     }
                 }
             }
@@ -425,18 +478,6 @@ __device__ __forceinline__ void fp64_lj_i(const double4* __restrict__ pos, int i
 // One FP32 pair of k_lj_mixed_bf: the rebasing shift from the entry's code, del, r^2 and, for a
 // fast pair (close2 <= r^2 < rc2_lo), its force added without a branch; returns whether the pair
 // takes the FP64 path (closer than close2, or within the window around the cutoff).
-__device__ __forceinline__ float mixed_del(uint32_t en, const float4& ri, const float4& rj, const LjArgs& a,
-                                           float& dx, float& dy, float& dz) {
-    const float sx = __int_as_float((int)((en & 0x03u) | 0x4B000000u)) - 8388609.0f;
-    const float sy = __int_as_float((int)((en & 0x0Cu) | 0x4B000000u)) - 8388612.0f;
-    const float sz = __int_as_float((int)((en & 0x30u) | 0x4B000000u)) - 8388624.0f;
-    dx = fmaf(a.hx, sx, ri.x - rj.x);
-    dy = fmaf(a.hy, sy, ri.y - rj.y);
-    dz = fmaf(a.hz, sz, ri.z - rj.z);
-    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-}
-__device__ __forceinline__ bool mixed_fast(float rsq, const LjArgs& a) { return rsq < a.rc2_lo && rsq >= a.close2; }
-
 template <bool THERMO>
 __device__ __forceinline__ bool mixed_pair(uint32_t en, const float4& ri, const float4& rj, const LjArgs& a,
                                            float& fx, float& fy, float& fz, float& ef, float& wf, int& ncnt) {

@@ -236,6 +236,29 @@ def test_mixed_force_error_dense(product, oracle):
         p.close()
 
 
+@pytest.mark.parametrize("half_mode", [0, 1])
+def test_mixed_half_list_force_error(product, oracle, half_mode):
+    """Mixed form over half lists (the reference's, and those keeping boundary pairs): the forces,
+    reactions included, within 1e-5 of rms of the FP64 half-list forces on the same positions
+    (15 steps: before the first rebuild, after which the reference's half lists let atoms overlap
+    across the boundary)."""
+    product.md_set_half_mode(half_mode)
+    p = make_sim(product, setup_lib=product, cells=(8, 8, 8), half=True)
+    try:
+        p.step(0.005, 15)
+        _, _, f64 = tinymd.full_state(product)
+        product.md_set_precision(1)
+        p.force()
+        product.md_final_integration(0.0)
+        _, _, f32 = tinymd.full_state(product)
+        err = rel_err(f32, f64)
+        assert err <= 1e-5, err
+    finally:
+        product.md_set_precision(0)
+        product.md_set_half_mode(0)
+        p.close()
+
+
 def test_half_lists_with_ghost_pairs(product, oracle):
     """Corrected half mode: lists equal the oracle's; forces equal the full-list forces."""
     product.md_set_half_mode(1)
