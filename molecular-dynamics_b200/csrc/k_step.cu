@@ -759,20 +759,23 @@ k_dem_mixed(const float4* __restrict__ pos32, const double4* __restrict__ pos, c
                 continue;
             }
             const double4 vj = ldg_d4(vel + j);
-            const float len = sqrtf(rsq);
-            if (!(len > 0.f)) continue;
+            // |del| and 1/|del| from one reciprocal square root (against a rounded square root and
+            // a division: the force 33.0 -> 28.9 us on the 48^3 FCC split)
+            if (!(rsq > 0.f)) continue;
+            const float inv = rsqrtf(rsq);
+            const float len = rsq * inv;
             const float delta = b.d2 - len;
-            const float inv = 1.0f / len;
             const float nx = dx * inv, ny = dy * inv, nz = dz * inv;
             const float rvx = vix - (float)vj.x, rvy = viy - (float)vj.y, rvz = viz - (float)vj.z;
             const float vn = rvx * nx + rvy * ny + rvz * nz;
             const float vtx = rvx - nx * vn, vty = rvy - ny * vn, vtz = rvz - nz * vn;
-            const float vtl = sqrtf(vtx * vtx + vty * vty + vtz * vtz);
+            const float vt2 = vtx * vtx + vty * vty + vtz * vtz;
+            const float tinv = vt2 > 0.f ? rsqrtf(vt2) : 0.f;
+            const float vtl = vt2 * tinv;
             float fn = b.k * delta - b.dn * vn;
             if (fn < 0.f) fn = 0.f;
             const float t1 = b.dt_ * vtl, t2 = b.mu * fn;
             const float ft = t1 < t2 ? t1 : t2;
-            const float tinv = vtl > 0.f ? 1.0f / vtl : 0.f;
             const float px = nx * fn - vtx * tinv * ft;
             const float py = ny * fn - vty * tinv * ft;
             const float pz = nz * fn - vtz * tinv * ft;

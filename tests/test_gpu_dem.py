@@ -83,7 +83,7 @@ def test_contact_model_fp64_bitwise(product, oracle, reset_dem):
 def test_contact_model_mixed_forces(product, reset_dem, cells):
     """Mixed form (FP32 pair arithmetic on rebased positions, FP64 at the contact and cutoff
     decisions): forces on the same state agree with the FP64 form's to 1e-4 of the rms force
-    (measured ~4e-5 and ~5e-5).  The normal force is k (2R - r) with overlaps of ~0.012 here:
+    (measured 4.6e-5 and 5.4e-5; 7.5e-5 at 48^3).  The normal force is k (2R - r) with overlaps of ~0.012 here:
     r carries ~1e-7 from the FP32 pair arithmetic, so the overlap itself is only good to
     ~1e-5 relative -- a cancellation that the LJ form does not have."""
     set_model(product, None, 1, 0.6)
