@@ -81,7 +81,10 @@ int md_write_grid_aabb_data_to_arrays(double *masses, struct Vector3D *positions
 /* anydsl_includes.h:20, core/grid.impala:323-358: bins locals and ghosts into
  * cells (a counting sort that also reorders the device arrays by cell). */
 void md_distribute_particles(void);
-/* anydsl_includes.h:21, core/neighborlist.impala:18-78 */
+/* anydsl_includes.h:21, core/neighborlist.impala:18-78.  Returns before the build's status (list
+ * overflow, locals outside the grid) is read: the next force starts on the new lists and the status
+ * is read while it runs, the build and force redone on an overflow; a warning of the build is
+ * latched by then, or by the next call that reads state or the error code. */
 void md_assemble_neighborlists(bool half_neighborlist, double cutoff_distance);
 /* anydsl_includes.h:22, core/runtime.impala:97-102 */
 void md_deallocate_grid(void);
