@@ -79,6 +79,44 @@ def test_atom_outside_the_grid(product, oracle):
     product.md_clear_error()
 
 
+def test_atom_outside_the_grid_at_a_later_build(product, oracle):
+    """The atom outside the grid again, now at a list build inside the run: the lists are built
+    without the periodic wrap (md_borders without md_enforce_pbc), so the atom stays outside; the
+    fused force kernel that the next md_initial_integration launches on those lists before their
+    status is read returns without writing, the outside atom's list is cleared and the kernel
+    runs again.  The states stay bit-identical to the oracle's, and the warning is latched."""
+    m, x, v, world, rank = tinymd.setup_particles("default", (6, 6, 6), lib=product)
+    x = x.copy()
+    x[0, 0] = world[1] + 5.0
+    p = make_sim(product, setup_lib=product, particles=(m, x, v, world, rank))
+    o = make_sim(oracle, setup_lib=product, particles=(m, x, v, world, rank))
+    try:
+        product.md_clear_error()
+        for sim in (p, o):
+            sim.step(0.005, 5)
+        for sim, lib in ((p, product), (o, oracle)):
+            sim.reneighbor(wrap=False)
+            sim.force()
+            lib.md_final_integration(0.005)
+            lib.md_initial_integration(0.005)
+            lib.md_synchronize_ghost_layer()
+            sim.force()
+            lib.md_final_integration(0.005)
+        assert product.md_last_error() == 5
+        product.md_clear_error()
+        for sim in (p, o):
+            sim.step(0.005, 10)
+        xp, vp, fp = tinymd.full_state(product)
+        xo, vo, fo = tinymd.full_state(oracle)
+        np.testing.assert_array_equal(xp, xo)
+        np.testing.assert_array_equal(vp, vo)
+        np.testing.assert_array_equal(fp, fo)
+    finally:
+        p.close()
+        o.close()
+        product.md_clear_error()
+
+
 @pytest.mark.parametrize("half,half_mode", [(False, 0), (True, 0), (True, 1)])
 def test_dense_cells(product, oracle, half, half_mode):
     """A compressed lattice (a = 1.1: ~66 atoms per cell, ~280 neighbours each) makes the list
