@@ -299,21 +299,25 @@ def test_half_lists_with_ghost_pairs(product, oracle):
 
 @pytest.mark.parametrize("precision", [0, 1])
 def test_131k_workload_stable_and_matches_oracle_lists(product, oracle, precision):
-    """The benchmark workload: lists equal the oracle's after reneighbouring; energy stays bounded."""
+    """The benchmark workload: lists equal the oracle's after reneighbouring, and in the FP64 form
+    positions, velocities and forces equal the oracle's bit for bit after 40 steps (two rebuilds);
+    energy stays bounded over 420 steps."""
     product.md_set_precision(precision)
     try:
         p = make_sim(product, setup_lib=product, cells=(32, 32, 32))
         o = make_sim(oracle, setup_lib=product, cells=(32, 32, 32))
-        p.step(0.005, 20)
-        o.step(0.005, 20)
+        p.step(0.005, 40)
+        o.step(0.005, 40)
         lp = tinymd.neighbor_lists(product, p.n)
         lo = tinymd.neighbor_lists(oracle, o.n)
         if precision == 0:
             for a, b in zip(lp, lo):
                 np.testing.assert_array_equal(a, b)
-            xp, vp, _ = tinymd.full_state(product)
-            xo, vo, _ = tinymd.full_state(oracle)
+            xp, vp, fp = tinymd.full_state(product)
+            xo, vo, fo = tinymd.full_state(oracle)
             np.testing.assert_array_equal(xp, xo)
+            np.testing.assert_array_equal(vp, vo)
+            np.testing.assert_array_equal(fp, fo)
         o.close()
         p.run(0.005, 380)
         _, v, _ = tinymd.full_state(product)
