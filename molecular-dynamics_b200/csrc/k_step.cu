@@ -60,7 +60,8 @@ __device__ __forceinline__ void put_partial(double* part, int q, double v, doubl
 // ---- prefetch ------------------------------------------------------------------------
 // The force kernels do not prefetch their list rows: a bulk L2 prefetch of every block's rows at
 // the start queued ~40 MB ahead of the first demand loads and cost 2.4 us (cold L2) and 1.4 us
-// (warm) per launch of the mixed kernel at 131k atoms; the quad loads one batch ahead suffice.
+// (warm) per launch of the mixed kernel at 131k atoms, and one of only the first 2-8 rows still
+// 0.5-0.9 us (cold); the quad loads one batch ahead suffice.
 
 // quad b of atom i's list (entries 4b .. 4b + 3)
 __device__ __forceinline__ uint4 list_quad(const uint32_t* nbl, int b, int i, int stride) {
