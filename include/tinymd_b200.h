@@ -98,14 +98,25 @@ void md_compute_lennard_jones(bool half_neighborlist, double cutoff_distance, do
 /* anydsl_includes.h:27, core/runtime.impala:203-247 */
 void md_compute_dem(bool half_neighborlist, double cutoff_distance, double damping_n, double damping_t,
                     double stiffness, double friction);
-/* anydsl_includes.h:28-29, core/runtime.impala:250-251 (one process: no-ops) */
+/* anydsl_includes.h:28-29, core/runtime.impala:250-251.  Several processes (one per GPU) form
+ * one run when the environment names the world size and this process's rank
+ * (TINYMD_WORLD_SIZE / TINYMD_RANK, else WORLD_SIZE / RANK as torchrun sets them, else
+ * OMPI_COMM_WORLD_SIZE / OMPI_COMM_WORLD_RANK, else PMI_SIZE / PMI_RANK): md_mpi_initialize
+ * connects them over TCP (rank 0 listens on TINYMD_ADDR or MASTER_ADDR, default 127.0.0.1,
+ * port TINYMD_PORT, else MASTER_PORT + 17, else 29417), selects this rank's GPU
+ * (TINYMD_DEVICE, else the launcher's local rank) and picks the transport of the halo data:
+ * NCCL when every rank has its own GPU, else page-locked host buffers over the TCP mesh
+ * (TINYMD_COMM=auto|socket|nccl).  Without those variables the run has one rank.
+ * md_mpi_finalize releases the grid and the connections.  Several ranks run full neighbour
+ * lists and exact ghosts; md_report_* print sums (times: maxima) over the ranks on rank 0. */
 void md_mpi_initialize(void);
 void md_mpi_finalize(void);
 /* anydsl_includes.h:30, comm/comm.impala:334-388 */
 void md_synchronize_ghost_layer(void);
 /* anydsl_includes.h:31, comm/comm.impala:528-642 */
 void md_borders(void);
-/* anydsl_includes.h:32, comm/comm.impala:392-525 (one process: no remote ranks, no-op) */
+/* anydsl_includes.h:32, comm/comm.impala:392-525 (one rank: nothing leaves; several: locals
+ * beyond the rank box move to the rank that owns their new place) */
 void md_exchange_particles(void);
 /* anydsl_includes.h:33-35, core/runtime.impala:258-264 (MPI buffers: stubs) */
 double md_get_send_buffer_value(int index);
@@ -120,7 +131,8 @@ int md_get_world_rank(void);
 /* anydsl_includes.h:40-41, core/runtime.impala:256-257 */
 int md_get_number_of_particles(void);
 int md_get_number_of_ghost_particles(void);
-/* anydsl_includes.h:42, core/runtime.impala:52-70 (one rank: the world box) */
+/* anydsl_includes.h:42, core/runtime.impala:52-70, comm/comm.impala:221-299 (the rank layout
+ * that minimises the ranks' surface, a periodic row-major cart; one rank: the world box) */
 void md_get_node_bounding_box(double const *world_aabb, double (*rank_aabb)[6]);
 /* anydsl_includes.h:43-44, core/runtime.impala:72-95, comm/lb.impala:52-86 (load balancing: stubs) */
 void md_compute_boundary_weights(double xmin, double xmax, double ymin, double ymax, double zmin, double zmax,
@@ -142,7 +154,8 @@ enum md_error {
     MD_ERR_ARGUMENT = 3,      /* invalid argument */
     MD_ERR_UNSUPPORTED = 4,   /* multi-process / load-balancing entry point */
     MD_ERR_OUT_OF_GRID = 5,   /* locals outside the cell grid at binning (warning; they get no neighbours) */
-    MD_ERR_NO_DEVICE = 6      /* no CUDA device */
+    MD_ERR_NO_DEVICE = 6,     /* no CUDA device */
+    MD_ERR_COMM = 7           /* the ranks could not connect, or an exchange between them failed */
 };
 int md_last_error(void);
 const char *md_last_error_string(void);
@@ -172,7 +185,8 @@ void md_set_thermo(int enable);
 /* out[0] = sum of pair energies 4 eps (s12 - s6) over list entries inside the
  * cutoff, out[1] = sum of f(r) r^2 over the same entries, out[2] = number of
  * list entries inside the cutoff, out[3] = sum of v.v of locals after the last
- * final integration.  Full lists count each pair twice. Returns 0 on success. */
+ * final integration.  Full lists count each pair twice.  With several ranks the sums are over
+ * all ranks (every rank calls).  Returns 0 on success. */
 int md_get_thermo(double *out);
 /* The same sums without waiting: md_thermo_request enqueues a copy of them (as of the work
  * issued so far) into page-locked memory and returns a ticket; md_thermo_fetch(ticket, out)
@@ -264,6 +278,22 @@ int tmd_setup_fetch(double *masses, struct Vector3D *positions, struct Vector3D 
 /* md_initialize_grid on the last generated setup. */
 int tmd_setup_initialize(double const *world, double const *rank, double cell_spacing, int cell_capacity,
                          int neighborlist_capacity);
+
+/* ---- rank layout and transport (several processes; md_mpi_initialize) ------ */
+/* comm/comm.impala:221-257: the rank grid dims[3] for `world` ranks over a box of side
+ * lengths len[3].  Returns 0, or -1 for world < 1. */
+int tmd_node_config(int world, double const *len, int *dims);
+/* The 26 regions around rank `rank` of the periodic row-major cart dims[3] (region
+ * t = ez*9 + ey*3 + ex - 1, e per axis 0 inside, 1 above, 2 below): peer[26] their owners,
+ * shift[26*3] the world lengths added to a position sent there, *selfmask the regions this
+ * rank owns itself.  Returns 0, or -1 for a rank outside the cart. */
+int tmd_topology(int rank, int const *dims, int *peer, int *shift, unsigned *selfmask);
+/* "none" (one rank), "socket" or "nccl": the transport of the halo data. */
+const char *tmd_comm_transport(void);
+/* Sum of v[n] over the ranks (rank order), on every rank.  Returns 0 or -1. */
+int tmd_comm_allreduce_sum(double *v, int n);
+/* One host message to rank `to` and one from rank `from` (bytes may be 0).  Returns 0 or -1. */
+int tmd_comm_sendrecv(int to, void const *sbuf, long long sbytes, int from, void *rbuf, long long rbytes);
 
 /* ---- differentiable form (adjoint) ---------------------------------------- */
 /* Trajectory: VV with LJ over full lists, exact periodic ghosts, neighbour

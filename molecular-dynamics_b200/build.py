@@ -25,10 +25,11 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I" + INC, "-I" + CSRC, "-I" + HOST]
-CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + INC, "-I" + HOST]
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-I" + INC, "-I" + HOST, "-I" + CSRC]
 
-CU_SOURCES = ["api.cu", "k_neigh.cu", "k_step.cu", "adjoint.cu", "noalloc.cu"]
-CPP_LIB_SOURCES = [os.path.join(CSRC, "setup_api.cpp"), os.path.join(HOST, "setups.cpp")]
+CU_SOURCES = ["api.cu", "k_neigh.cu", "k_step.cu", "k_halo.cu", "adjoint.cu", "noalloc.cu"]
+CPP_LIB_SOURCES = [os.path.join(CSRC, "setup_api.cpp"), os.path.join(HOST, "setups.cpp"), os.path.join(CSRC, "comm.cpp")]
+CUDA_INC = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "include")
 HEADERS = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))] + \
           [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith(".h")] + \
           [os.path.join(INC, "tinymd_b200.h")]
@@ -63,11 +64,11 @@ def build(verbose=False):
     for path in CPP_LIB_SOURCES:
         obj = os.path.join(OBJ, os.path.basename(path) + ".o")
         if _stale(obj, [path] + HEADERS):
-            _run([CXX] + CXXFLAGS + ["-c", "-o", obj, path])
+            _run([CXX] + CXXFLAGS + ["-I" + CUDA_INC, "-c", "-o", obj, path])
         objs.append(obj)
     so = os.path.join(LIB, "libtinymd_b200.so")
     if _stale(so, objs):
-        _run([NVCC] + ARCH + ["-shared", "-Xlinker", "-Bsymbolic", "-o", so] + objs)
+        _run([NVCC] + ARCH + ["-shared", "-Xlinker", "-Bsymbolic", "-o", so] + objs + ["-ldl"])
     md = os.path.join(LIB, "md")
     main = os.path.join(HOST, "main.cpp")
     if os.path.exists(main) and _stale(md, [so, main] + HEADERS):

@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "md_common.cuh"
+#include "comm.h"
 #include "md_state.h"
 #include "tinymd_b200.h"
 
@@ -407,6 +408,10 @@ using namespace tmd;
 extern "C" {
 
 int md_adjoint_configure(int steps, int reneigh, double dt, double cutoff, double skin, int precision) {
+    if (comm().active()) {  // the trajectory is one rank's periodic box
+        set_error(MD_ERR_UNSUPPORTED, "md_adjoint_configure: the differentiable form runs on one rank");
+        return -1;
+    }
     if (steps < 1 || reneigh < 1 || !(dt > 0) || !(cutoff > 0) || skin < 0) {
         set_error(MD_ERR_ARGUMENT, "md_adjoint_configure: invalid arguments");
         return -1;

@@ -15,6 +15,7 @@
 #include <deque>
 #include <vector>
 
+#include "comm.h"
 #include "md_common.cuh"
 #include "md_state.h"
 #include "tinymd_b200.h"
@@ -310,7 +311,7 @@ bool grow_atoms(State& s, int need) {
     s.slab = slab;
     s.img_ok = 0;
     s.capA = newc;
-    if (oldc > 0) std::printf("0> reallocate_particle_capacity(): %d\n", newc);
+    if (oldc > 0) std::printf("%d> reallocate_particle_capacity(): %d\n", comm().rank(), newc);
     return true;
 }
 
@@ -324,6 +325,25 @@ void grow_lists(State& s, int rows) {
     s.lists_valid = 0;
 }
 
+// A rank's local count changes when atoms migrate: the border masks and counts and the list
+// stride follow it (contents are not kept: every user writes them anew after a migration).
+bool ensure_locals(State& s, int n) {
+    n = std::max(n, 1);
+    const int nblk = border_blocks(n);
+    if (n > s.nb_stride) {
+        s.nb_stride = ((n + n / 8 + 31) / 32) * 32;
+        dfree(&s.nbl);
+        dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+        dfree(&s.bmask);
+        dalloc(&s.bmask, (size_t)s.nb_stride);
+        dfree(&s.bcount);
+        dalloc(&s.bcount, (size_t)2 * 27 * border_blocks(s.nb_stride) + 1);
+        s.lists_valid = 0;
+    }
+    ensure_scan_scratch(s, 27 * nblk);
+    return s.nbl && s.bmask && s.bcount;
+}
+
 namespace {
 
 bool allocate_state(State& s, int N, int nb_cap) {
@@ -333,10 +353,11 @@ bool allocate_state(State& s, int N, int nb_cap) {
     const int nseg = 2 * (ncells + 1);
     dalloc(&s.cnt, nseg + 1);
     dalloc(&s.cstart, nseg + 1);
-    dalloc(&s.bmask, (size_t)std::max(N, 1));
-    const int nblk = border_blocks(std::max(N, 1));
-    dalloc(&s.bcount, (size_t)2 * 26 * nblk + 1);
+    // sized by the list stride (at least N), which ensure_locals grows with the local count
     s.nb_stride = ((std::max(N, 1) + 31) / 32) * 32;
+    dalloc(&s.bmask, (size_t)s.nb_stride);
+    const int nblk = border_blocks(s.nb_stride);
+    dalloc(&s.bcount, (size_t)2 * 27 * nblk + 1);  // border types (26) or migration classes (27), scanned
     s.nb_cap = list_rows(nb_cap > 0 ? nb_cap : 100);
     dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
     if (!s.ev_counted) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_counted, cudaEventDisableTiming));
@@ -653,6 +674,25 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
         return -1;
     }
     if (s.alive) md_deallocate_grid();
+    Comm& cm = comm();
+    if (cm.active()) {
+        // several ranks: the layout of md_get_node_bounding_box (made here from the world box
+        // when the caller skipped it); every divided axis must hold a full halo per rank
+        if (!cm.topo_set) {
+            double len[3];
+            int dims[3];
+            for (int d = 0; d < 3; ++d) len[d] = aabb[2 * d + 1] - aabb[2 * d];
+            node_config(cm.world(), len, dims);
+            make_topology(cm.world(), cm.rank(), dims, cm.topo);
+            cm.topo_set = true;
+        }
+        for (int d = 0; d < 3; ++d)
+            if (cm.topo.dims[d] > 1 && rank_aabb[2 * d + 1] - rank_aabb[2 * d] < cell_spacing) {
+                set_error(MD_ERR_ARGUMENT, "md_initialize_grid: a rank box is narrower than the cell spacing "
+                                           "(too many ranks for this box)");
+                return -1;
+            }
+    }
     TMD_CUDA(cudaGetDevice(&s.device));
     if (!s.stream && !s.stream_set) {
         TMD_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
@@ -677,6 +717,8 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
 
     s.N = n;
     s.G = 0;
+    s.halo.on = cm.active();
+    if (s.halo.on) s.ghost_exact = 1;  // ghosts of other ranks are exact images; own ones likewise
     s.pc = s.vc = s.ac = 0;
     s.lists_valid = 0;
     s.pend_init = false;
@@ -717,10 +759,16 @@ void md_create_velocity(double t_request) {
     if (!require_alive("md_create_velocity")) return;
     materialize_mirror(s);
     const int n = s.N;
+    Comm& cm = comm();
+    long long ntot = n;
     double vt[3] = {0.0, 0.0, 0.0};
     for (int i = 0; i < n; ++i)
         for (int d = 0; d < 3; ++d) vt[d] = vt[d] + s.h_vel[3 * i + d];
-    for (int d = 0; d < 3; ++d) vt[d] = vt[d] / (double)n;
+    if (cm.active() && !(cm.allreduce_sum(&ntot, 1) && cm.allreduce_sum(vt, 3))) {
+        set_error(MD_ERR_COMM, "md_create_velocity: " + cm.error());
+        return;
+    }
+    for (int d = 0; d < 3; ++d) vt[d] = vt[d] / (double)ntot;
     // the mean removed and core/thermo.impala:1-16's sum taken in the same pass (same terms in
     // the same order as a separate pass over the updated velocities)
     double t = 0.0;
@@ -729,7 +777,11 @@ void md_create_velocity(double t_request) {
         for (int d = 0; d < 3; ++d) v[d] = v[d] - vt[d];
         t += (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * 1.0;
     }
-    t = t * (1.0 / (double)(n * 3 - 3));
+    if (cm.active() && !cm.allreduce_sum(&t, 1)) {
+        set_error(MD_ERR_COMM, "md_create_velocity: " + cm.error());
+        return;
+    }
+    t = t * (1.0 / (double)(ntot * 3 - 3));
     double factor = std::sqrt(t_request / t);
     for (int i = 0; i < n; ++i)
         for (int d = 0; d < 3; ++d) s.h_vel[3 * i + d] = s.h_vel[3 * i + d] * factor;
@@ -785,8 +837,17 @@ void md_copy_data_from_accelerator(void) {
     s.mirror_na = NA;
 }
 
-void md_exchange_particles(void) {  // comm/comm.impala:392-525: no remote ranks in one process
-    if (require_alive("md_exchange_particles")) flush_locals(g_state);
+// comm/comm.impala:392-525: with one rank nothing leaves (the periodic wrap is md_enforce_pbc's);
+// with several, locals beyond the rank box move to their new owner (k_halo.cu)
+void md_exchange_particles(void) {
+    State& s = g_state;
+    if (!require_alive("md_exchange_particles")) return;
+    flush_locals(s);
+    if (s.halo.on) {
+        s.pend_ghost = false;  // every ghost is written anew by the border pass that follows
+        phase_mark(PH_COMM);
+        run_migrate(s);
+    }
 }
 
 void md_enforce_pbc(void) {  // wraps locals only: a pending ghost carry stays pending
@@ -818,6 +879,12 @@ void md_distribute_particles(void) {
 void md_assemble_neighborlists(bool half, double cutoff) {
     State& s = g_state;
     if (!require_alive("md_assemble_neighborlists")) return;
+    if (half && s.halo.on) {
+        // a half list leaves the reaction on a ghost of another rank, which would need the
+        // forces sent back: several ranks run full lists
+        set_error(MD_ERR_UNSUPPORTED, "md_assemble_neighborlists: half lists on several ranks (use full lists)");
+        return;
+    }
     // pending ghost links stay pending when nothing else is (the list build then runs them as
     // extra blocks); any other pending work may read them, so then they go first, alone
     const bool hold = s.pend_links && !s.pend_force.valid && !s.pend_final && !s.pend_ghost && !s.pend_init &&
@@ -875,6 +942,10 @@ void md_synchronize_ghost_layer(void) {
     } else {
         phase_mark(PH_COMM);
         run_ghost_sync(s);
+    }
+    if (s.halo.on) {
+        phase_mark(PH_COMM);
+        run_halo_sync(s);
     }
 }
 
@@ -1025,6 +1096,7 @@ void md_deallocate_grid(void) {
     fold_prof(true);
     phase_reset();
     free_all(s);
+    halo_free(s);
     release_adjoint();
     s.mirror_pending = 0;
     s.alive = false;
@@ -1066,28 +1138,39 @@ void md_print_ghost(void) {
     std::fflush(stdout);
 }
 
-void md_mpi_initialize(void) {}
-void md_mpi_finalize(void) {}
-void md_barrier(void) {  // no other ranks: wait for this rank's device work
+// core/runtime.impala:250-251: the ranks of the environment connect (comm.cpp); one rank when
+// the environment names none
+void md_mpi_initialize(void) {
+    if (!comm().init()) set_error(MD_ERR_COMM, "md_mpi_initialize: " + comm().error());
+}
+void md_mpi_finalize(void) {
+    if (g_state.alive) md_deallocate_grid();
+    comm().finalize();
+}
+void md_barrier(void) {  // this rank's device work done, then every rank's
     State& s = g_state;
     if (s.alive) {
         flush_all(s);
         sync_stream(s);
     }
+    if (comm().active() && !comm().barrier()) set_error(MD_ERR_COMM, "md_barrier: " + comm().error());
 }
-int md_get_world_size(void) { return 1; }
-int md_get_world_rank(void) { return 0; }
+int md_get_world_size(void) { return comm().world(); }
+int md_get_world_rank(void) { return comm().rank(); }
 int md_get_number_of_particles(void) { return g_state.N; }
 int md_get_number_of_ghost_particles(void) { return g_state.G; }
 
-// comm/comm.impala:254-331 with one rank
+// comm/comm.impala:221-299: the rank layout that minimises the ranks' surface, this rank's
+// place in the periodic cart and its box (one rank: the world box)
 void md_get_node_bounding_box(double const* aabb, double (*rank)[6]) {
-    for (int d = 0; d < 3; ++d) {
-        double len = (aabb[2 * d + 1] - aabb[2 * d]) / 1.0;
-        double lo = aabb[2 * d] + len * 0.0;
-        (*rank)[2 * d] = lo;
-        (*rank)[2 * d + 1] = lo + len;
-    }
+    Comm& cm = comm();
+    double len[3];
+    int dims[3];
+    for (int d = 0; d < 3; ++d) len[d] = aabb[2 * d + 1] - aabb[2 * d];
+    node_config(cm.world(), len, dims);
+    make_topology(cm.world(), cm.rank(), dims, cm.topo);
+    cm.topo_set = true;
+    rank_box(aabb, dims, cm.topo.coords, *rank);
 }
 
 // load balancing / multi-process entry points (out of scope on one GPU)
@@ -1154,8 +1237,12 @@ void md_report_iterations(void) {
         if (s.force_cfg.valid) s.rsq_iters = count_pairs_inside(s, s.force_cfg.rc);
     }
     s.force_iters = total;
+    long long it[3] = {s.force_iters, s.rsq_iters, s.integration_iters};
+    Comm& cm = comm();
+    if (cm.active() && !cm.allreduce_sum(it, 3)) set_error(MD_ERR_COMM, "md_report_iterations: " + cm.error());
+    if (cm.rank() != 0) return;  // the sums are printed once (core/runtime.impala:280-296)
     std::printf("ForceIters RsqIters IntegrationIters\n");
-    std::printf("%lld %lld %lld \n", s.force_iters, s.rsq_iters, s.integration_iters);
+    std::printf("%lld %lld %lld \n", it[0], it[1], it[2]);
     std::fflush(stdout);
 }
 
@@ -1166,6 +1253,26 @@ void md_report_particles(void) {
         flush_all(s);
         materialize_mirror(s, 1);
     }
+    Comm& cm = comm();
+    if (cm.active()) {  // sums over the ranks, printed once (core/runtime.impala:298-316)
+        long long ng[2] = {s.N, s.G};
+        double t = 0.0;
+        for (int i = 0; i < s.N; ++i) {
+            const double* v = &s.h_vel[(size_t)i * 3];
+            t += (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) * 1.0;
+        }
+        if (!(cm.allreduce_sum(ng, 2) && cm.allreduce_sum(&t, 1))) {
+            set_error(MD_ERR_COMM, "md_report_particles: " + cm.error());
+            return;
+        }
+        if (cm.rank() != 0) return;
+        std::printf("# Local # Ghost Temp\n");
+        std::printf("%lld %lld ", ng[0], ng[1]);
+        print_g(t * (1.0 / (double)(ng[0] * 3 - 3)));
+        std::printf("\n");
+        std::fflush(stdout);
+        return;
+    }
     std::printf("# Local # Ghost Temp\n");
     std::printf("%d %d ", s.N, s.G);
     print_g(host_temperature(s));
@@ -1174,9 +1281,12 @@ void md_report_particles(void) {
 }
 
 // core/runtime.impala:318-337
-void md_report_time(double total, double force, double neigh, double comm, double lb, double other) {
+void md_report_time(double total, double force, double neigh, double comm_t, double lb, double other) {
+    double v[6] = {total, force, neigh, comm_t, lb, other};
+    Comm& cm = comm();  // the slowest rank's times, printed once
+    if (cm.active() && !cm.allreduce_max(v, 6)) set_error(MD_ERR_COMM, "md_report_time: " + cm.error());
+    if (cm.rank() != 0) return;
     std::printf("Total Force Neigh Comm Balance Other\n");
-    double v[6] = {total, force, neigh, comm, lb, other};
     for (double x : v) {
         print_g(x);
         std::printf(" ");
@@ -1208,7 +1318,7 @@ void md_set_half_mode(int ghost_pairs) {
 }
 void md_set_ghost_mode(int exact) {
     if (g_state.alive) flush_all(g_state);
-    g_state.ghost_exact = exact ? 1 : 0;
+    g_state.ghost_exact = (exact || g_state.halo.on) ? 1 : 0;  // several ranks: exact ghosts only
 }
 void md_set_dem_model(int fixed, double radius) {
     if (g_state.alive) flush_all(g_state);
@@ -1226,6 +1336,10 @@ int md_get_thermo(double* out) {
     TMD_CUDA(cudaMemcpyAsync(out, s.thermo_dev, 4 * sizeof(double), cudaMemcpyDeviceToHost, s.stream));
     sync_stream(s);
     s.rsq_iters = (long long)out[2];
+    if (comm().active() && !comm().allreduce_sum(out, 4)) {  // every rank's sums
+        set_error(MD_ERR_COMM, "md_get_thermo: " + comm().error());
+        return -1;
+    }
     return 0;
 }
 // Asynchronous thermo: the sums as of the work enqueued so far go to a page-locked slot by a
@@ -1254,6 +1368,10 @@ int md_thermo_fetch(int ticket, double* out) {
     TMD_CUDA(cudaEventSynchronize(s.thermo_ev[k]));
     for (int q = 0; q < 4; ++q) out[q] = s.thermo_host[4 * k + q];
     s.rsq_iters = (long long)out[2];
+    if (comm().active() && !comm().allreduce_sum(out, 4)) {  // every rank fetches the same tickets
+        set_error(MD_ERR_COMM, "md_thermo_fetch: " + comm().error());
+        return -1;
+    }
     return 0;
 }
 void md_synchronize(void) {

@@ -24,6 +24,7 @@
 
 #include <cstdio>
 
+#include "comm.h"
 #include "md_common.cuh"
 #include "md_state.h"
 
@@ -173,12 +174,23 @@ __global__ void __launch_bounds__(kBorderThreads) k_border_count(double4* __rest
 
 // Pass 2 (after an exclusive scan of bcount into boff): writes every ghost at
 // slot N + g, g its reference ghost index, with its source / root links.
+// MR (several ranks): only the types in selfmask are periodic ghosts of this rank; the others
+// are images for the neighbour ranks, listed (root, type) in type order for the halo pack.
+// tab[t] / tab[26 + t]: images of the other kind before type t (k_halo.cu's table).
+struct RemoteOut {
+    const int* tab;
+    int* send_ref;
+    int* send_type;
+    unsigned selfmask;
+};
+
+template <bool MR>
 __global__ void __launch_bounds__(kBorderThreads) k_border_emit(double4* __restrict__ pos, double4* __restrict__ vel, double4* __restrict__ frc,
                               double* __restrict__ mass, int* __restrict__ ref, int* __restrict__ slot_of_ref,
                               const unsigned* __restrict__ bmask, const int* __restrict__ boff,
                               int* __restrict__ gsrc, int* __restrict__ groot, int* __restrict__ gcode,
                               int* __restrict__ bsrc_ref, int* __restrict__ broot_ref, int* __restrict__ bcode,
-                              int N, int nblk, int capA, GeoArgs a, int sync_vel) {
+                              int N, int nblk, int capA, GeoArgs a, int sync_vel, RemoteOut ro) {
     __shared__ int wpre[kBorderThreads / 32][26];
     __shared__ unsigned char s_rank[26][kBorderThreads];  // a thread's rank among its warp's ghosts of each type
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -210,7 +222,13 @@ __global__ void __launch_bounds__(kBorderThreads) k_border_emit(double4* __restr
     auto gidx = [&](int t) { return boff[t * nblk + blockIdx.x] + wpre[wid][t] + s_rank[t][threadIdx.x]; };
     for (int t = 0; t < 26; ++t) {
         if (!((m >> t) & 1u)) continue;
-        const int g = gidx(t);
+        if (MR && !((ro.selfmask >> t) & 1u)) {
+            const int k = gidx(t) - ro.tab[26 + t];
+            ro.send_ref[k] = r;
+            ro.send_type[k] = t;
+            continue;
+        }
+        const int g = gidx(t) - (MR ? ro.tab[t] : 0);
         const int slot = N + g;
         if (slot >= capA) continue;  // the host grows the arrays and redoes the pass
         const int tt = t + 1;
@@ -231,7 +249,7 @@ __global__ void __launch_bounds__(kBorderThreads) k_border_emit(double4* __restr
         }
         // source of the last pass: the ghost of the same root without the last axis, or the root
         const int tsrc = tt - e[last] * (last == 0 ? 1 : (last == 1 ? 3 : 9));
-        const int src_ref = tsrc == 0 ? r : N + gidx(tsrc - 1);
+        const int src_ref = tsrc == 0 ? r : N + gidx(tsrc - 1) - (MR ? ro.tab[tsrc - 1] : 0);
         const int src_slot = tsrc == 0 ? s_root : src_ref;  // a ghost's slot is its reference index
         int code = 0;
         for (int d = 0; d < 3; ++d) {
@@ -361,6 +379,12 @@ struct LinkArgs {
 __device__ __forceinline__ void ghost_link(int h, const LinkArgs& l) {
     const int N = l.N, capA = l.capA;
     int g = l.ref[N + h] - N;
+    if (l.broot_ref[g] < 0) {  // received from another rank: refreshed by the halo exchange
+        l.gsrc[h] = l.groot[h] = -1;
+        l.gcode[h] = 0;
+        l.rref[N + h] = -1;
+        return;
+    }
     const int s1 = l.slot_of_ref[l.bsrc_ref[g]];
     const int r = l.slot_of_ref[l.broot_ref[g]];
     l.gsrc[h] = s1;
@@ -775,12 +799,48 @@ void run_borders(State& s, bool wrap) {
     GeoArgs a = geo_args(s.geo);
     const int N = s.N;
     const int nblk = border_blocks(N);
-    if (N == 0) {
+    if (N == 0 && !s.halo.on) {
         s.G = 0;
         return;
     }
     prof_begin(K_BORDER);
     const int nseg = 2 * (a.ncells + 1);
+    const int n = 26 * nblk;
+    // boff = exclusive scan of bcount, stored after the counts
+    int* boff = s.bcount + n;
+    if (s.halo.on) {
+        // several ranks: the per-type totals first (they split the images into this rank's
+        // periodic ghosts and the ones for other ranks), then the emit, then the exchange;
+        // a rank without locals still takes part in the exchange
+        if (N > 0) {
+            if (wrap)
+                k_border_count<true><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref,
+                                                                  s.bmask, s.bcount, N, nblk, a, s.cnt, nseg,
+                                                                  s.status_dev);
+            else
+                k_border_count<false><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref,
+                                                                   s.bmask, s.bcount, N, nblk, a, s.cnt, nseg,
+                                                                   s.status_dev);
+            s.bin_zeroed = true;
+            launched(K_BORDER);
+            exclusive_scan(s, s.bcount, boff, n);
+        }
+        bool ok = halo_plan_borders(s, N > 0 ? boff : nullptr, nblk);
+        if (ok && N + s.halo.gself > s.capA) ok = grow_atoms(s, N + s.halo.gself);
+        if (ok && N > 0) {
+            RemoteOut ro{s.halo.tab, s.halo.send_ref, s.halo.send_type, comm().topo.selfmask};
+            k_border_emit<true><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac],
+                                                             s.mass.b[s.ac], s.ref.b[s.ac], s.slot_of_ref, s.bmask, boff,
+                                                             s.gsrc, s.groot, s.gcode, s.bsrc_ref, s.broot_ref,
+                                                             s.bcode, N, nblk, s.capA, a, s.dem_fixed, ro);
+            launched(K_BORDER);
+        }
+        if (ok) ok = halo_finish_borders(s);
+        if (!ok) s.G = 0;
+        prof_end(K_BORDER);
+        s.lists_valid = 0;
+        return;
+    }
     if (wrap)
         k_border_count<true><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.img.b[s.ac], s.slot_of_ref, s.bmask,
                                                           s.bcount, N, nblk, a, s.cnt, nseg, s.status_dev);
@@ -789,9 +849,6 @@ void run_borders(State& s, bool wrap) {
                                                            s.bcount, N, nblk, a, s.cnt, nseg, s.status_dev);
     s.bin_zeroed = true;
     launched(K_BORDER);
-    const int n = 26 * nblk;
-    // boff = exclusive scan of bcount, stored after the counts
-    int* boff = s.bcount + n;
     exclusive_scan(s, s.bcount, boff, n);
     // The ghost count comes back while the emit kernel already runs: emit writes only the
     // slots below the capacity, so when the count shows the capacity was short the host
@@ -804,10 +861,10 @@ void run_borders(State& s, bool wrap) {
     TMD_CUDA(cudaMemcpyAsync(&s.status_host->nghost, boff + n, sizeof(int), cudaMemcpyDeviceToHost, s.copy_stream));
     TMD_CUDA(cudaEventRecord(s.ev_counted, s.copy_stream));
     auto emit = [&]() {
-        k_border_emit<<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
+        k_border_emit<false><<<nblk, kBorderThreads, 0, s.stream>>>(s.pos.b[s.pc], s.vel.b[s.vc], s.frc.b[s.ac], s.mass.b[s.ac],
                                                   s.ref.b[s.ac], s.slot_of_ref, s.bmask, boff, s.gsrc, s.groot,
                                                   s.gcode, s.bsrc_ref, s.broot_ref, s.bcode, N, nblk, s.capA,
-                                                  a, s.dem_fixed);
+                                                  a, s.dem_fixed, RemoteOut{nullptr, nullptr, nullptr, 0u});
         launched(K_BORDER);
     };
     emit();

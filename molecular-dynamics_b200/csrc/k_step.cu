@@ -850,8 +850,9 @@ k_integrate(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, cons
         if (DEMV) vel_n[t] = vel_o[t];
         return;
     }
-    const int code = gcode[g];
     const int s = GM == 1 ? gsrc[g] : groot[g];
+    if (s < 0) return;  // a ghost received from another rank: the halo exchange refreshes it
+    const int code = gcode[g];
     double4 xs;
     if (s < a.N) {
         double4 vs = vel_o[s];
@@ -896,8 +897,9 @@ k_ghost_sync(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, con
     }
     if (t >= a.N + a.G) return;
     const int g = t - a.N;
-    const int code = gcode[g];
     const int s = GM == 1 ? gsrc[g] : groot[g];
+    if (s < 0) return;  // received from another rank (halo exchange)
+    const int code = gcode[g];
     const double4 xs = pos_o[s];
     const int base = GM == 1 ? 0 : 8;
     double4 x;
@@ -927,8 +929,9 @@ k_ghost_refresh(const double4* __restrict__ pos_o, double4* __restrict__ pos_n, 
         if (MIXED) pos32_n[t] = pos32_o[t];
         return;
     }
-    const int code = gcode[g];
     const int s = GM == 1 ? gsrc[g] : groot[g];
+    if (s < 0) return;  // received from another rank (halo exchange)
+    const int code = gcode[g];
     const double4 xs = s < a.N ? pos_n[s] : pos_o[s];
     const int base = GM == 1 ? 0 : 8;
     double4 x;

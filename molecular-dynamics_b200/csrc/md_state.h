@@ -116,6 +116,29 @@ constexpr int kThermoSlots = 8;  // asynchronous thermo reads in flight at most
 constexpr int kBorderThreads = 1024;
 inline int border_blocks(int N) { return (N + kBorderThreads - 1) / kBorderThreads; }
 
+// Multi-rank runs (comm.h): the images this rank sends into its neighbours' regions and the
+// ghosts it receives from them.  Ghost order: the periodic images of this rank's own atoms
+// (gself, the border pass's order), then the received ghosts peer by peer (ascending rank),
+// each peer's in its send order.
+struct Halo {
+    bool on = false;          // more than one rank
+    int gself = 0;            // ghosts that are images of this rank's own atoms
+    int nsend = 0, nrecv = 0; // images sent / ghosts received by the last border pass
+    int send_cap = 0;
+    int* send_ref = nullptr;  // [send_cap] root reference index of each image sent, by region type
+    int* send_type = nullptr; // its region type
+    int* pk_ref = nullptr;    // the same in message order (peer by peer): the per-step packing
+    int* pk_type = nullptr;
+    int* tab = nullptr;       // [kHaloTab] device copy of the per-type offsets (see k_halo.cu)
+    int* tab_host = nullptr;  // pinned: offsets read back, then the table to upload
+    double* sbuf = nullptr;   // device message buffers
+    double* rbuf = nullptr;
+    size_t sbuf_cap = 0, rbuf_cap = 0;  // doubles
+    HostVec hs, hr;           // page-locked staging when the transport is host sockets
+    std::vector<int> send_cnt, recv_cnt;  // per peer rank (Topology::peers), at the last border pass
+};
+constexpr int kHaloTab = 128;
+
 struct PendingForce {
     bool valid = false;
     bool dem = false;
@@ -248,6 +271,8 @@ struct State {
     bool build_zeroed = false;  // likewise the list-build status, by the binning's reorder kernel
     bool pend_links = false;    // ghost links of the last binning not yet launched (see flush_links)
 
+    Halo halo;  // multi-rank only
+
     // reported iteration counters (core/runtime.impala:3-5)
     long long force_iters = 0, rsq_iters = 0, integration_iters = 0;
     int last_force_half = 0;
@@ -311,6 +336,16 @@ bool force_init_fusable(const State& s, const PendingForce& p);
 // them over, 1 is the reference two-phase refresh, 2 exact images
 void run_ghost_refresh(State& s, int gm);
 void run_reduce_thermo(State& s, int nblocks, int nq);
+// multi-rank (k_halo.cu): atoms that left the rank box go to their new owners (the caller
+// flushed pending work); the remote part of a border pass (after its emit); the ghosts
+// received from other ranks refreshed from the current positions of their roots
+bool run_migrate(State& s);
+bool halo_plan_borders(State& s, const int* boff, int nblk);
+bool halo_finish_borders(State& s);
+bool run_halo_sync(State& s);
+void halo_free(State& s);
+// the per-local arrays sized by the local count (border masks and counts, list stride) hold n
+bool ensure_locals(State& s, int n);
 // sums the [q][nblocks] per-block partials of quantities q0..q1-1 into thermo_dev[q]
 void run_reduce_partials(State& s, int nblocks, int q0, int q1);
 void exclusive_scan(State& s, const int* in, int* out, int n);

@@ -98,6 +98,11 @@ _EXTENSION_API = {
     "tmd_setup_generate": (_c_int, [_c_int, _vp, _vp, _vp, _vp, _c_double]),
     "tmd_setup_fetch": (_c_int, [_vp, _vp, _vp]),
     "tmd_setup_initialize": (_c_int, [_vp, _vp, _c_double, _c_int, _c_int]),
+    "tmd_node_config": (_c_int, [_c_int, _vp, _vp]),
+    "tmd_topology": (_c_int, [_c_int, _vp, _vp, _vp, _vp]),
+    "tmd_comm_transport": (ctypes.c_char_p, []),
+    "tmd_comm_allreduce_sum": (_c_int, [_vp, _c_int]),
+    "tmd_comm_sendrecv": (_c_int, [_c_int, _vp, _c_ll, _c_int, _vp, _c_ll]),
     "md_adjoint_configure": (_c_int, [_c_int, _c_int, _c_double, _c_double, _c_double, _c_int]),
     "md_adjoint_forward": (_c_int, [_vp, _c_double, _c_double, _vp]),
     "md_adjoint_backward": (_c_int, [_vp, _vp, _vp]),

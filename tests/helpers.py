@@ -1,4 +1,9 @@
 """Helpers shared by the tests: run the same setup on the product and the oracle."""
+import os
+import socket
+import subprocess
+import sys
+
 import numpy as np
 
 import tinymd
@@ -23,3 +28,32 @@ def rel_err(a, b):
     """max |a-b| / rms(b) over all components."""
     rms = np.sqrt(np.mean(np.asarray(b) ** 2))
     return float(np.max(np.abs(np.asarray(a) - np.asarray(b))) / (rms if rms > 0 else 1.0))
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def run_ranks(world, argv, env_extra=None, timeout=120):
+    """Starts `world` processes of argv (each argument formatted with rank=r) as the ranks of one
+    run (TINYMD_WORLD_SIZE / TINYMD_RANK / TINYMD_PORT); returns [(returncode, output)]."""
+    port = free_port()
+    procs = []
+    for r in range(world):
+        env = dict(os.environ, TINYMD_WORLD_SIZE=str(world), TINYMD_RANK=str(r), TINYMD_PORT=str(port),
+                   TINYMD_COMM_TIMEOUT="60")
+        env.update(env_extra or {})
+        procs.append(subprocess.Popen([a.format(rank=r) for a in argv], env=env, stdout=subprocess.PIPE,
+                                      stderr=subprocess.STDOUT, text=True))
+    outs = []
+    for p in procs:
+        try:
+            out, _ = p.communicate(timeout=timeout)
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            raise
+        outs.append((p.returncode, out))
+    return outs

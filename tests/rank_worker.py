@@ -1,0 +1,92 @@
+"""One rank of a multi-process run, started by the rank tests (not collected by pytest).
+
+    python tests/rank_worker.py comm OUT.json
+        md_mpi_initialize over the environment's ranks, then the transport's collectives,
+        a ring of messages, md_get_node_bounding_box and md_barrier (no GPU needed).
+    python tests/rank_worker.py md OUT.npz CELLS STEPS PRECISION [REBUILD]
+        the md driver's sequence (main.cpp:614-776 of tinyMD) on this rank's part of the
+        default FCC lattice: setup inside the rank box, velocities, borders, lists, LJ forces,
+        STEPS timesteps with reneighbouring every REBUILD steps; saves the locals and the
+        neighbour counts of the first lists.
+
+The environment names the world size and rank (TINYMD_WORLD_SIZE / TINYMD_RANK) and the
+rendezvous port (TINYMD_PORT).
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "molecular-dynamics_b200"))
+import tinymd  # noqa: E402
+from tinymd import ptr  # noqa: E402
+
+
+def comm_mode(out):
+    lib = tinymd.load(build_if_missing=False)
+    lib.md_mpi_initialize()
+    err = lib.md_last_error()
+    res = {"err": err, "msg": lib.md_last_error_string().decode()}
+    if err == 0:
+        w, r = lib.md_get_world_size(), lib.md_get_world_rank()
+        res.update(world=w, rank=r, transport=lib.tmd_comm_transport().decode())
+        v = np.array([float(r), 1.5, -2.0 * r])
+        res["allreduce_rc"] = lib.tmd_comm_allreduce_sum(ptr(v), 3)
+        res["allreduce"] = v.tolist()
+        # a ring of 1 MiB messages (larger than a socket buffer)
+        n = 1 << 17
+        send = np.arange(n, dtype=np.float64) + 1000.0 * r
+        recv = np.zeros(n)
+        res["ring_rc"] = lib.tmd_comm_sendrecv((r + 1) % w, ptr(send), send.nbytes, (r - 1) % w, ptr(recv),
+                                               recv.nbytes)
+        res["ring_ok"] = bool(np.array_equal(recv, np.arange(n, dtype=np.float64) + 1000.0 * ((r - 1) % w)))
+        world = np.array([0.0, 12.0, 0.0, 10.0, -1.0, 9.0])
+        box = np.zeros(6)
+        lib.md_get_node_bounding_box(ptr(world), ptr(box))
+        res["box"] = box.tolist()
+        lib.md_barrier()
+        res["err_after"] = lib.md_last_error()
+        lib.md_mpi_finalize()
+    with open(out, "w") as f:
+        json.dump(res, f)
+
+
+def md_mode(out, cells, steps, precision, rebuild):
+    lib = tinymd.load(build_if_missing=False)
+    lib.md_mpi_initialize()
+    tinymd.check(lib)
+    rank = lib.md_get_world_rank()
+    grid = np.array([cells] * 3, dtype=np.int32)
+    potmin, dt = 1.6796, 0.005
+    world, a1, a2 = np.zeros(6), np.zeros(6), np.zeros(6)
+    assert lib.tmd_setup_world(0, ptr(grid), potmin, ptr(world), ptr(a1), ptr(a2)) == 0
+    box = np.zeros(6)
+    lib.md_get_node_bounding_box(ptr(world), ptr(box))
+    n = lib.tmd_setup_generate(0, ptr(world), ptr(box), ptr(a1), ptr(a2), potmin)
+    m, x, v = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3))
+    lib.tmd_setup_fetch(ptr(m), ptr(x), ptr(v))
+    lib.md_set_precision(precision)
+    sim = tinymd.Simulation(lib, m, x, v, world, box, temp=1.44, reneigh=rebuild)
+    sizes = np.zeros(lib.md_get_number_of_particles(), dtype=np.int32)
+    # neighbour counts of the first lists, by the locals' positions (identical to the setup's)
+    _, x0, _, _ = sim.arrays()
+    lists = tinymd.neighbor_lists(lib, len(sizes))
+    sizes = np.array([len(l) for l in lists], dtype=np.int32)
+    sim.step(dt, steps)
+    nloc, ngh = sim.counts()
+    sim.n = nloc
+    _, x1, v1, f1 = sim.arrays()
+    tinymd.check(lib)
+    np.savez(out, x0=x0, nb0=sizes, x=x1, v=v1, f=f1, n=nloc, g=ngh, rank=rank, box=box,
+             transport=lib.tmd_comm_transport().decode())
+    sim.close()
+    lib.md_mpi_finalize()
+
+
+if __name__ == "__main__":
+    if sys.argv[1] == "comm":
+        comm_mode(sys.argv[2])
+    else:
+        md_mode(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]),
+                int(sys.argv[6]) if len(sys.argv) > 6 else 10)

@@ -1,0 +1,136 @@
+"""Several ranks on one GPU against the one-box oracle (comm/comm.impala's decomposition).
+
+Each rank is its own process (tests/rank_worker.py md) and owns the atoms of its box of the
+default FCC lattice (8^3 cells, 2,048 atoms); the ranks exchange halos and migrate atoms
+through the library (host-socket transport: the processes share the device, so no kernel
+of one waits for another's).  The oracle runs the same setup as one box with exact ghosts.
+
+* At the first lists every atom has the oracle's neighbour count (integer-exact), and the
+  union of the ranks' atoms is the oracle's lattice.
+* After 100 steps with a rebuild (migration + borders) every 10, every atom's position,
+  velocity and force matches the oracle's to 1e-9 (FP64: only the summation order differs,
+  since a rank's lists hold its ghosts in another order), and the atom count is conserved.
+* The mixed form on four ranks stays within the FP32 tolerance of the same run.
+* The reference's own driver (main.cpp, unmodified, linked to the product) runs on two ranks.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+from scipy.spatial import cKDTree
+
+from conftest import ORACLE_LIB, ROOT
+from helpers import run_ranks
+
+sys.path.insert(0, os.path.join(ROOT, "molecular-dynamics_b200"))
+import tinymd  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+WORKER = os.path.join(ROOT, "tests", "rank_worker.py")
+REF_B200 = os.path.join(ROOT, "oracle", "_ref", "refmd_b200")
+OUR_MD = os.path.join(ROOT, "molecular-dynamics_b200", "lib", "md")
+CELLS, STEPS, REBUILD, DT = 8, 100, 10, 0.005
+
+
+@pytest.fixture(scope="module")
+def one_box():
+    lib = tinymd.load()
+    olib = tinymd.open_library(ORACLE_LIB)
+    olib.oracle_set_ghost_mode(1)
+    m, x, v, world, rank = tinymd.setup_particles("default", (CELLS,) * 3, lib=lib)
+    sim = tinymd.Simulation(olib, m, x, v, world, rank, temp=1.44, reneigh=REBUILD)
+    nb0 = np.array([len(l) for l in tinymd.neighbor_lists(olib, sim.n)])
+    sim.step(DT, STEPS)
+    _, x1, v1, f1 = sim.arrays()
+    sim.close()
+    olib.oracle_set_ghost_mode(0)
+    box = np.array([world[1] - world[0], world[3] - world[2], world[5] - world[4]])
+    return dict(x0=x, nb0=nb0, x=x1, v=v1, f=f1, box=box, lo=np.array(world[0::2]))
+
+
+def run(world, tmp_path, precision=0, steps=STEPS):
+    outs = run_ranks(world, [sys.executable, WORKER, "md", str(tmp_path / "r{rank}.npz"), str(CELLS), str(steps),
+                             str(precision), str(REBUILD)],
+                     {"TINYMD_COMM": "socket", "TINYMD_DEVICE": "0"}, timeout=600)
+    for rc, out in outs:
+        assert rc == 0, out
+    return [dict(np.load(tmp_path / f"r{r}.npz")) for r in range(world)]
+
+
+def match(ref_x, x, box, lo):
+    """Index of the nearest reference atom (periodic) for each row of x, and its distance."""
+    tree = cKDTree(np.mod(ref_x - lo, box), boxsize=box)
+    d, i = tree.query(np.mod(x - lo, box))
+    return i, d
+
+
+@pytest.mark.parametrize("world", [2, 4, 8])
+def test_ranks_match_the_one_box_oracle(one_box, tmp_path, world):
+    res = run(world, tmp_path)
+    assert all(str(r["transport"]) == "socket" for r in res)
+    # the first lists: the ranks' atoms are the lattice, each with the oracle's neighbour count
+    x0 = np.concatenate([r["x0"] for r in res])
+    nb0 = np.concatenate([r["nb0"] for r in res])
+    assert len(x0) == len(one_box["x0"])
+    key = {tuple(p): k for k, p in enumerate(one_box["x0"])}
+    idx = np.array([key[tuple(p)] for p in x0])
+    assert len(set(idx.tolist())) == len(idx)
+    assert np.array_equal(nb0, one_box["nb0"][idx])
+    # after the run
+    n = sum(int(r["n"]) for r in res)
+    assert n == len(one_box["x"])
+    x = np.concatenate([r["x"] for r in res])
+    v = np.concatenate([r["v"] for r in res])
+    f = np.concatenate([r["f"] for r in res])
+    i, d = match(one_box["x"], x, one_box["box"], one_box["lo"])
+    assert len(set(i.tolist())) == n
+    assert d.max() < 1e-9
+    np.testing.assert_allclose(v, one_box["v"][i], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(f, one_box["f"][i], rtol=0, atol=1e-8)
+    # atoms did migrate: some rank's final count differs from its initial one
+    assert any(int(r["n"]) != len(r["x0"]) for r in res)
+
+
+def test_mixed_form_on_four_ranks(one_box, tmp_path):
+    res = run(4, tmp_path, precision=1)
+    x = np.concatenate([r["x"] for r in res])
+    f = np.concatenate([r["f"] for r in res])
+    i, d = match(one_box["x"], x, one_box["box"], one_box["lo"])
+    assert len(set(i.tolist())) == len(one_box["x"])
+    assert d.max() < 1e-5
+    rms = np.sqrt(np.mean(one_box["f"] ** 2))
+    assert np.max(np.abs(f - one_box["f"][i])) / rms < 1e-3
+
+
+def test_reference_driver_on_two_ranks(tmp_path):
+    """The reference's main.cpp on two ranks reports what this repository's md driver reports on
+    one rank with exact ghosts (several ranks run exact ghosts): the same atom count,
+    temperature (six digits) and iteration counts."""
+    if not os.path.exists(REF_B200):
+        pytest.skip("oracle/_ref/refmd_b200 not built (make -C oracle refmd needs the reference tree)")
+    args = ["-x", "8", "-y", "8", "-z", "8", "-s", "100"]
+    one = subprocess.run([OUR_MD] + args + ["--ghost", "exact"], capture_output=True, text=True, cwd=tmp_path,
+                         timeout=600)
+    assert one.returncode == 0, one.stdout + one.stderr
+    outs = run_ranks(2, [REF_B200] + args, {"TINYMD_COMM": "socket", "TINYMD_DEVICE": "0"}, timeout=600)
+    for rc, out in outs:
+        assert rc == 0, out
+
+    def report(lines, head):
+        for k, line in enumerate(lines):
+            if line.startswith(head) and k + 1 < len(lines):
+                return lines[k + 1].split()
+        return None
+
+    r1 = report(one.stdout.splitlines(), "# Local")
+    r2 = report(outs[0][1].splitlines(), "# Local")  # rank 0 prints the sums over the ranks
+    assert report(outs[1][1].splitlines(), "# Local") is None
+    assert r1 is not None and r2 is not None
+    assert r2[0] == r1[0] == "2048"
+    assert abs(float(r2[2]) - float(r1[2])) <= 1e-5 * float(r1[2])
+    it1 = report(one.stdout.splitlines(), "ForceIters")
+    it2 = report(outs[0][1].splitlines(), "ForceIters")
+    assert it1 == it2
