@@ -3,11 +3,12 @@
     python tests/rank_worker.py comm OUT.json
         md_mpi_initialize over the environment's ranks, then the transport's collectives,
         a ring of messages, md_get_node_bounding_box and md_barrier (no GPU needed).
-    python tests/rank_worker.py md OUT.npz CELLS STEPS PRECISION [REBUILD]
-        the md driver's sequence (main.cpp:614-776 of tinyMD) on this rank's part of the
-        default FCC lattice: setup inside the rank box, velocities, borders, lists, LJ forces,
-        STEPS timesteps with reneighbouring every REBUILD steps; saves the locals and the
-        neighbour counts of the first lists.
+    python tests/rank_worker.py md OUT.npz CELLS STEPS PRECISION [REBUILD] [BENCHMARK]
+        the md driver's sequence (main.cpp:614-776 of tinyMD) on this rank's part of a setup
+        (default: the FCC lattice with LJ forces; granular_gas_fcc: the contact-fixed DEM
+        configuration): setup inside the rank box, velocities, borders, lists, forces, STEPS
+        timesteps with reneighbouring every REBUILD steps; saves the locals and the neighbour
+        counts of the first lists.
 
 The environment names the world size and rank (TINYMD_WORLD_SIZE / TINYMD_RANK) and the
 rendezvous port (TINYMD_PORT).
@@ -52,27 +53,38 @@ def comm_mode(out):
         json.dump(res, f)
 
 
-def md_mode(out, cells, steps, precision, rebuild):
+# the DEM benchmark configuration (contact-fixed model, radius 0.6): damping_n, damping_t,
+# stiffness, friction
+DEM = (0.1, 0.1, 100.0, 0.5)
+
+
+def md_mode(out, cells, steps, precision, rebuild, benchmark="default"):
     lib = tinymd.load(build_if_missing=False)
     lib.md_mpi_initialize()
     tinymd.check(lib)
     rank = lib.md_get_world_rank()
     grid = np.array([cells] * 3, dtype=np.int32)
-    potmin, dt = 1.6796, 0.005
+    potmin = 1.6796
+    dem = benchmark == "granular_gas_fcc"
+    dt = 0.001 if dem else 0.005
     world, a1, a2 = np.zeros(6), np.zeros(6), np.zeros(6)
-    assert lib.tmd_setup_world(0, ptr(grid), potmin, ptr(world), ptr(a1), ptr(a2)) == 0
+    b = tinymd.BENCHMARKS[benchmark]
+    assert lib.tmd_setup_world(b, ptr(grid), potmin, ptr(world), ptr(a1), ptr(a2)) == 0
     box = np.zeros(6)
     lib.md_get_node_bounding_box(ptr(world), ptr(box))
-    n = lib.tmd_setup_generate(0, ptr(world), ptr(box), ptr(a1), ptr(a2), potmin)
+    n = lib.tmd_setup_generate(b, ptr(world), ptr(box), ptr(a1), ptr(a2), potmin)
     m, x, v = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3))
     lib.tmd_setup_fetch(ptr(m), ptr(x), ptr(v))
     lib.md_set_precision(precision)
-    sim = tinymd.Simulation(lib, m, x, v, world, box, temp=1.44, reneigh=rebuild)
-    sizes = np.zeros(lib.md_get_number_of_particles(), dtype=np.int32)
-    # neighbour counts of the first lists, by the locals' positions (identical to the setup's)
+    if dem:
+        lib.md_set_dem_model(1, 0.6)
+        sim = tinymd.Simulation(lib, m, x, v, world, box, cutoff=1.2, skin=0.3, force_field="dem", dem=DEM,
+                                reneigh=rebuild)
+    else:
+        sim = tinymd.Simulation(lib, m, x, v, world, box, temp=1.44, reneigh=rebuild)
+    # the first lists' neighbour counts, in the locals' reference order (the setup's order)
     _, x0, _, _ = sim.arrays()
-    lists = tinymd.neighbor_lists(lib, len(sizes))
-    sizes = np.array([len(l) for l in lists], dtype=np.int32)
+    sizes = np.array([len(l) for l in tinymd.neighbor_lists(lib, sim.n)], dtype=np.int32)
     sim.step(dt, steps)
     nloc, ngh = sim.counts()
     sim.n = nloc
@@ -89,4 +101,4 @@ if __name__ == "__main__":
         comm_mode(sys.argv[2])
     else:
         md_mode(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]),
-                int(sys.argv[6]) if len(sys.argv) > 6 else 10)
+                int(sys.argv[6]) if len(sys.argv) > 6 else 10, sys.argv[7] if len(sys.argv) > 7 else "default")
