@@ -340,6 +340,7 @@ int main(int argc, char** argv) {
         std::cout << "- Ghost refresh: " << ghost << std::endl << std::endl;
     }
     const bool vtk = !vtk_dir.empty();
+    if (vtk && md_get_world_size() > 1) vtk_dir += std::to_string(md_get_world_rank());  // main.cpp:654-659
     if (vtk) vtk_dir += "/";
 
     PhaseClock timer((size_t)runs);

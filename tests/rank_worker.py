@@ -80,8 +80,9 @@ def md_mode(out, cells, steps, precision, rebuild, benchmark="default"):
         lib.md_set_dem_model(1, 0.6)
         sim = tinymd.Simulation(lib, m, x, v, world, box, cutoff=1.2, skin=0.3, force_field="dem", dem=DEM,
                                 reneigh=rebuild)
-    else:
-        sim = tinymd.Simulation(lib, m, x, v, world, box, temp=1.44, reneigh=rebuild)
+    else:  # main.cpp:664-667: velocities are created for the lattice setups only
+        temp = 1.44 if benchmark in ("default", "half") else None
+        sim = tinymd.Simulation(lib, m, x, v, world, box, temp=temp, reneigh=rebuild)
     # the first lists' neighbour counts, in the locals' reference order (the setup's order)
     _, x0, _, _ = sim.arrays()
     sizes = np.array([len(l) for l in tinymd.neighbor_lists(lib, sim.n)], dtype=np.int32)

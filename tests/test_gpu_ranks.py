@@ -95,6 +95,43 @@ def test_ranks_match_the_one_box_oracle(one_box, tmp_path, world):
     assert any(int(r["n"]) != len(r["x0"]) for r in res)
 
 
+@pytest.mark.parametrize("bench,cells,world", [("default", 8, 3), ("default", 8, 6), ("half", 10, 4),
+                                               ("body_collision", 6, 4)])
+def test_other_layouts_and_sparse_setups(tmp_path, bench, cells, world):
+    """Layouts whose rank boxes are not powers of two of the lattice (1x1x3, 1x2x3), the half
+    setup on 1x2x2 (the upper ranks start without atoms and receive the ones that expand into
+    them) and body_collision (two bodies in a mostly empty box), 100 steps against the one-box
+    oracle."""
+    from helpers import make_sim
+    lib = tinymd.load()
+    olib = tinymd.open_library(ORACLE_LIB)
+    olib.oracle_set_ghost_mode(1)
+    try:
+        o = make_sim(olib, benchmark=bench, cells=(cells,) * 3, setup_lib=lib, reneigh=REBUILD)
+        o.step(DT, STEPS)
+        _, xo, vo, fo = o.arrays()
+        o.close()
+    finally:
+        olib.oracle_set_ghost_mode(0)
+    outs = run_ranks(world, [sys.executable, WORKER, "md", str(tmp_path / "r{rank}.npz"), str(cells), str(STEPS), "0",
+                             str(REBUILD), bench], {"TINYMD_COMM": "socket", "TINYMD_DEVICE": "0"}, timeout=600)
+    for rc, out in outs:
+        assert rc == 0, out
+    res = [dict(np.load(tmp_path / f"r{r}.npz")) for r in range(world)]
+    if bench == "half":
+        assert any(len(r["x0"]) == 0 for r in res) and all(int(r["n"]) > 0 for r in res)
+    x = np.concatenate([r["x"] for r in res])
+    v = np.concatenate([r["v"] for r in res])
+    f = np.concatenate([r["f"] for r in res])
+    _, _, _, wbox, _ = tinymd.setup_particles(bench, (cells,) * 3, lib=lib)
+    box = np.array([wbox[1] - wbox[0], wbox[3] - wbox[2], wbox[5] - wbox[4]])
+    i, d = match(xo, x, box, np.array(wbox[0::2]))
+    assert len(x) == len(xo) and len(set(i.tolist())) == len(xo)
+    assert d.max() < 1e-9
+    np.testing.assert_allclose(v, vo[i], rtol=0, atol=1e-9)
+    np.testing.assert_allclose(f, fo[i], rtol=0, atol=1e-8)
+
+
 def test_contact_dem_on_two_ranks(tmp_path):
     """The contact-fixed DEM model (ghosts carry their root's velocity, so the halo does too) on
     the granular-gas FCC setup, two ranks against the one-box oracle."""
