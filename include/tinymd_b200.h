@@ -288,6 +288,9 @@ int tmd_node_config(int world, double const *len, int *dims);
  * shift[26*3] the world lengths added to a position sent there, *selfmask the regions this
  * rank owns itself.  Returns 0, or -1 for a rank outside the cart. */
 int tmd_topology(int rank, int const *dims, int *peer, int *shift, unsigned *selfmask);
+/* This rank's halo at the last border pass: out[0] its own periodic ghosts, out[1] images sent
+ * per step, out[2] ghosts received per step, out[3] neighbour ranks.  Returns -1 on one rank. */
+int tmd_halo_info(int *out);
 /* "none" (one rank), "socket" or "nccl": the transport of the halo data. */
 const char *tmd_comm_transport(void);
 /* Sum of v[n] over the ranks (rank order), on every rank.  Returns 0 or -1. */

@@ -1587,6 +1587,17 @@ int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double 
     return s.last_error == MD_ERR_CUDA ? -1 : 0;
 }
 
+// several ranks: this rank's own periodic ghosts, images sent and ghosts received per step,
+// neighbour ranks (the halo's size: (sent + received) x 24 bytes per step)
+int tmd_halo_info(int* out) {
+    const Halo& h = g_state.halo;
+    out[0] = h.gself;
+    out[1] = h.nsend;
+    out[2] = h.nrecv;
+    out[3] = (int)comm().topo.peers.size();
+    return h.on ? 0 : -1;
+}
+
 int md_get_grid_info(int* out) {
     State& s = g_state;
     out[0] = s.geo.nx;

@@ -9,6 +9,9 @@
         configuration): setup inside the rank box, velocities, borders, lists, forces, STEPS
         timesteps with reneighbouring every REBUILD steps; saves the locals and the neighbour
         counts of the first lists.
+    python tests/rank_worker.py perf OUT.json CELLS STEPS REBUILD PRECISION
+        the LJ lattice timed over STEPS native timesteps (md_run_timesteps) after warm-up: host
+        time per step, the device phase split and this rank's halo size.
 
 The environment names the world size and rank (TINYMD_WORLD_SIZE / TINYMD_RANK) and the
 rendezvous port (TINYMD_PORT).
@@ -97,9 +100,52 @@ def md_mode(out, cells, steps, precision, rebuild, benchmark="default"):
     lib.md_mpi_finalize()
 
 
+def perf_mode(out, cells, steps, rebuild, precision):
+    """The LJ lattice split over the ranks, timed through md_run_timesteps (host clock, after
+    warm-up), with the device phase split and this rank's halo size."""
+    import time
+    lib = tinymd.load(build_if_missing=False)
+    lib.md_mpi_initialize()
+    tinymd.check(lib)
+    grid = np.array([cells] * 3, dtype=np.int32)
+    potmin = 1.6796
+    world, a1, a2 = np.zeros(6), np.zeros(6), np.zeros(6)
+    assert lib.tmd_setup_world(0, ptr(grid), potmin, ptr(world), ptr(a1), ptr(a2)) == 0
+    box = np.zeros(6)
+    lib.md_get_node_bounding_box(ptr(world), ptr(box))
+    n = lib.tmd_setup_generate(0, ptr(world), ptr(box), ptr(a1), ptr(a2), potmin)
+    m, x, v = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3))
+    lib.tmd_setup_fetch(ptr(m), ptr(x), ptr(v))
+    lib.md_set_precision(precision)
+    sim = tinymd.Simulation(lib, m, x, v, world, box, temp=1.44, reneigh=rebuild)
+    sim.run(0.005, 2 * rebuild)  # warm-up
+    lib.md_barrier()
+    lib.md_set_phase_timing(1)
+    t0 = time.perf_counter()
+    sim.run(0.005, steps)
+    lib.md_barrier()
+    t1 = time.perf_counter()
+    ph = np.zeros(6)
+    lib.md_get_phase_times(ptr(ph))
+    halo = np.zeros(4, dtype=np.int32)
+    lib.tmd_halo_info(ptr(halo))
+    nloc, ngh = sim.counts()
+    res = {"rank": lib.md_get_world_rank(), "world": lib.md_get_world_size(),
+           "transport": lib.tmd_comm_transport().decode(), "n": nloc, "g": ngh, "gself": int(halo[0]),
+           "nsend": int(halo[1]), "nrecv": int(halo[2]), "peers": int(halo[3]),
+           "us_per_step": (t1 - t0) / steps * 1e6, "phase_ms": ph.tolist()}
+    tinymd.check(lib)
+    with open(out, "w") as f:
+        json.dump(res, f)
+    sim.close()
+    lib.md_mpi_finalize()
+
+
 if __name__ == "__main__":
     if sys.argv[1] == "comm":
         comm_mode(sys.argv[2])
+    elif sys.argv[1] == "perf":
+        perf_mode(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]), int(sys.argv[6]))
     else:
         md_mode(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]),
                 int(sys.argv[6]) if len(sys.argv) > 6 else 10, sys.argv[7] if len(sys.argv) > 7 else "default")
