@@ -291,6 +291,9 @@ int tmd_topology(int rank, int const *dims, int *peer, int *shift, unsigned *sel
 /* This rank's halo at the last border pass: out[0] its own periodic ghosts, out[1] images sent
  * per step, out[2] ghosts received per step, out[3] neighbour ranks.  Returns -1 on one rank. */
 int tmd_halo_info(int *out);
+/* The NCCL binding on this GPU alone: a one-rank communicator sends `bytes` to itself through the
+ * calls the halo exchange uses.  0 on a match, -2 when libnccl.so.2 is absent, -1 otherwise. */
+int tmd_comm_nccl_selftest(long long bytes);
 /* "none" (one rank), "socket" or "nccl": the transport of the halo data. */
 const char *tmd_comm_transport(void);
 /* Sum of v[n] over the ranks (rank order), on every rank.  Returns 0 or -1. */

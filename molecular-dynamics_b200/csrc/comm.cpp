@@ -28,6 +28,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 namespace tmd {
 
@@ -95,8 +96,6 @@ void rank_box(const double w[6], const int dims[3], const int coords[3], double 
 }
 
 // ---- NCCL, opened at run time ----------------------------------------------------------------
-namespace {
-
 struct Nccl {
     void* so = nullptr;
     ncclResult_t (*get_unique_id)(ncclUniqueId*) = nullptr;
@@ -133,6 +132,8 @@ struct Nccl {
     }
 };
 Nccl g_nccl;
+
+namespace {
 
 // ---- sockets -------------------------------------------------------------------------------------
 double now_s() {
@@ -581,6 +582,40 @@ int tmd_topology(int rank, int const* dims, int* peer, int* shift, unsigned* sel
 }
 
 const char* tmd_comm_transport(void) { return tmd::comm().transport(); }
+
+// The NCCL binding on this process's GPU alone: a one-rank communicator sends `bytes` of a device
+// buffer to itself through the same group / send / receive calls the halo exchange issues, on a
+// stream, and the copy is compared.  0 when it matches, -2 without libnccl, -1 otherwise.
+int tmd_comm_nccl_selftest(long long bytes) {
+    using tmd::g_nccl;
+    if (bytes <= 0 || !g_nccl.open()) return bytes <= 0 ? -1 : -2;
+    ncclUniqueId id;
+    ncclComm_t c = nullptr;
+    if (g_nccl.get_unique_id(&id) != ncclSuccess || g_nccl.init_rank(&c, 1, id, 0) != ncclSuccess) return -1;
+    const size_t n = (size_t)bytes;
+    std::vector<unsigned char> h(n), back(n, 0);
+    for (size_t i = 0; i < n; ++i) h[i] = (unsigned char)(i * 131u + 7u);
+    void *a = nullptr, *b = nullptr;
+    cudaStream_t st = nullptr;
+    bool ok = cudaMalloc(&a, n) == cudaSuccess && cudaMalloc(&b, n) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMemcpy(a, h.data(), n, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMemset(b, 0, n) == cudaSuccess;
+    if (ok) {
+        ncclResult_t e = g_nccl.group_start();
+        if (e == ncclSuccess) e = g_nccl.send(a, n, ncclChar, 0, c, st);
+        if (e == ncclSuccess) e = g_nccl.recv(b, n, ncclChar, 0, c, st);
+        const ncclResult_t e2 = g_nccl.group_end();
+        ok = e == ncclSuccess && e2 == ncclSuccess && cudaStreamSynchronize(st) == cudaSuccess &&
+             cudaMemcpy(back.data(), b, n, cudaMemcpyDeviceToHost) == cudaSuccess && back == h;
+    }
+    g_nccl.destroy(c);
+    if (st) cudaStreamDestroy(st);
+    if (a) cudaFree(a);
+    if (b) cudaFree(b);
+    cudaGetLastError();
+    return ok ? 0 : -1;
+}
 
 int tmd_comm_allreduce_sum(double* v, int n) { return tmd::comm().allreduce_sum(v, n) ? 0 : -1; }
 

@@ -102,6 +102,7 @@ _EXTENSION_API = {
     "tmd_topology": (_c_int, [_c_int, _vp, _vp, _vp, _vp]),
     "tmd_comm_transport": (ctypes.c_char_p, []),
     "tmd_halo_info": (_c_int, [_vp]),
+    "tmd_comm_nccl_selftest": (_c_int, [_c_ll]),
     "tmd_comm_allreduce_sum": (_c_int, [_vp, _c_int]),
     "tmd_comm_sendrecv": (_c_int, [_c_int, _vp, _c_ll, _c_int, _vp, _c_ll]),
     "md_adjoint_configure": (_c_int, [_c_int, _c_int, _c_double, _c_double, _c_double, _c_int]),

@@ -9,6 +9,8 @@
         configuration): setup inside the rank box, velocities, borders, lists, forces, STEPS
         timesteps with reneighbouring every REBUILD steps; saves the locals and the neighbour
         counts of the first lists.
+    python tests/rank_worker.py nccl BYTES
+        the NCCL binding on this process's GPU alone (tmd_comm_nccl_selftest).
     python tests/rank_worker.py perf OUT.json CELLS STEPS REBUILD PRECISION
         the LJ lattice timed over STEPS native timesteps (md_run_timesteps) after warm-up: host
         time per step, the device phase split and this rank's halo size.
@@ -144,6 +146,10 @@ def perf_mode(out, cells, steps, rebuild, precision):
 if __name__ == "__main__":
     if sys.argv[1] == "comm":
         comm_mode(sys.argv[2])
+    elif sys.argv[1] == "nccl":  # the NCCL binding on this GPU alone (one-rank communicator)
+        rc = tinymd.load(build_if_missing=False).tmd_comm_nccl_selftest(int(sys.argv[2]))
+        print("nccl selftest", rc)
+        sys.exit(0 if rc == 0 else 1)
     elif sys.argv[1] == "perf":
         perf_mode(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]), int(sys.argv[6]))
     else:

@@ -178,6 +178,16 @@ def test_mixed_form_on_four_ranks(one_box, tmp_path):
     assert np.max(np.abs(f - one_box["f"][i])) / rms < 1e-2
 
 
+def test_nccl_binding_on_one_gpu():
+    """The NCCL transport's calls (libnccl opened at run time, a communicator, a send/receive
+    group on a stream) carry a device buffer to the same rank: the binding works on this GPU.
+    Two ranks over NCCL need two GPUs."""
+    env = dict(os.environ, NCCL_SOCKET_IFNAME=os.environ.get("NCCL_SOCKET_IFNAME", "lo"))
+    r = subprocess.run([sys.executable, WORKER, "nccl", str(3 << 20)], capture_output=True, text=True, timeout=300,
+                       env=env)
+    assert r.returncode == 0, r.stdout + r.stderr
+
+
 def test_reference_driver_on_two_ranks(tmp_path):
     """The reference's main.cpp on two ranks reports what this repository's md driver reports on
     one rank with exact ghosts (several ranks run exact ghosts): the same atom count,
