@@ -242,6 +242,8 @@ void free_all(State& s) {
     dfree(&s.slab);
     int** ip[] = {&s.cnt, &s.cstart, &s.bcount, &s.scan_part};
     for (int** q : ip) dfree(q);
+    dfree(&s.lb_tiles);
+    s.lb_tile_cap = 0;
     s.img_ok = 0;
     s.ghosts_pushed = 0;
     dfree(&s.bmask);

@@ -750,6 +750,85 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_single(const int* __restr
 }
 
 // ---- host wrappers ---------------------------------------------------------------
+// Single-pass exclusive scan of a long array (decoupled look-back): block b scans tile b,
+// publishes its total, then adds the totals of the tiles before it -- a tile that already
+// knows its inclusive prefix ends the walk -- and publishes that prefix.  A tile word holds
+// (launch epoch << 2 | state) << 32 | value, so nothing is reset between launches.  The wait
+// for a predecessor is bounded: past the limit the block sums that predecessor's inputs (and
+// all before it) directly, so the result never depends on the wait ending (the grids here
+// are a few dozen blocks, all resident at once).  One launch with ~11 blocks for the 21k cell
+// counts of a 131k-atom rebuild, where one block walked all of them.
+constexpr int kLbThreads = 256, kLbItems = 8, kLbTile = kLbThreads * kLbItems;
+constexpr int kLbSpinLimit = 1 << 14;  // polls of a predecessor's word (64 ns apart) before summing it directly
+
+__device__ __forceinline__ unsigned long long lb_word(unsigned epoch, unsigned state, int v) {
+    return ((unsigned long long)((epoch << 2) | state) << 32) | (unsigned)v;
+}
+
+__global__ void __launch_bounds__(kLbThreads)
+k_scan_lookback(const int* __restrict__ in, int* __restrict__ out, int n, int ntiles,
+                unsigned long long* __restrict__ tiles, unsigned epoch) {
+    __shared__ int sh[32];
+    __shared__ int s_prefix, s_missing;
+    const int tile = blockIdx.x;
+    const int base = tile * kLbTile + threadIdx.x * kLbItems;
+    int v[kLbItems];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kLbItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0;
+        sum += v[k];
+    }
+    int total;
+    const int ex = block_exscan(sum, &total, sh);
+    if (threadIdx.x == 0) {
+        int excl = 0, missing = -1;
+        volatile unsigned long long* tw = tiles;
+        if (tile == 0) {
+            tw[0] = lb_word(epoch, 2u, total);
+        } else {
+            tw[tile] = lb_word(epoch, 1u, total);
+            const unsigned want = epoch & 0x3fffffffu;
+            for (int j = tile - 1; j >= 0; --j) {
+                unsigned long long w = tw[j];
+                int spins = 0;
+                while (((unsigned)(w >> 34) != want || ((w >> 32) & 3u) == 0u) && spins < kLbSpinLimit) {
+                    __nanosleep(64);
+                    w = tw[j];
+                    ++spins;
+                }
+                if ((unsigned)(w >> 34) != want || ((w >> 32) & 3u) == 0u) {
+                    missing = j;
+                    break;
+                }
+                excl += (int)(unsigned)w;
+                if (((w >> 32) & 3u) == 2u) break;
+            }
+            if (missing < 0) tw[tile] = lb_word(epoch, 2u, excl + total);
+        }
+        s_prefix = excl;
+        s_missing = missing;
+    }
+    __syncthreads();
+    int prefix = s_prefix;
+    if (s_missing >= 0) {  // the inputs of tiles 0..missing summed directly
+        const int end = min(n, (s_missing + 1) * kLbTile);
+        int part = 0;
+        for (int i = threadIdx.x; i < end; i += kLbThreads) part += in[i];
+        int all;
+        block_exscan(part, &all, sh);
+        prefix += all;
+        if (threadIdx.x == 0) ((volatile unsigned long long*)tiles)[tile] = lb_word(epoch, 2u, prefix + total);
+    }
+    int e = prefix + ex;
+#pragma unroll
+    for (int k = 0; k < kLbItems; ++k) {
+        if (base + k < n) out[base + k] = e;
+        e += v[k];
+    }
+    if (tile == ntiles - 1 && threadIdx.x == 0) out[n] = prefix + total;
+}
+
 static inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
 
 void ensure_scan_scratch(State& s, int n) {
@@ -761,8 +840,35 @@ void ensure_scan_scratch(State& s, int n) {
     }
 }
 
+// look-back scans from this many values on (below, one block is as fast)
+#ifndef TMD_LB_MIN
+#define TMD_LB_MIN 8192
+#endif
+constexpr int kLookbackMin = TMD_LB_MIN;
+
+static bool ensure_lookback(State& s, int ntiles) {
+    if (ntiles <= s.lb_tile_cap) return true;
+    dfree(&s.lb_tiles);
+    s.lb_tile_cap = ntiles + 64;
+    dalloc(&s.lb_tiles, s.lb_tile_cap);
+    if (!s.lb_tiles) {
+        s.lb_tile_cap = 0;
+        return false;
+    }
+    TMD_CUDA(cudaMemsetAsync(s.lb_tiles, 0, sizeof(unsigned long long) * s.lb_tile_cap, s.stream));
+    return true;
+}
+
 // out[0..n-1] = exclusive prefix sums of in, out[n] = total (in != out allowed only)
 void exclusive_scan(State& s, const int* in, int* out, int n) {
+    if (n >= kLookbackMin) {
+        const int ntiles = nblocks(n, kLbTile);
+        if (ensure_lookback(s, ntiles)) {
+            k_scan_lookback<<<ntiles, kLbThreads, 0, s.stream>>>(in, out, n, ntiles, s.lb_tiles, ++s.lb_epoch);
+            launched(K_SCAN);
+            return;
+        }
+    }
     if (n <= kScanSingleMax) {
         if (s.scan_attr_device != s.device) {  // a function attribute is set per device
             TMD_CUDA(cudaFuncSetAttribute(k_scan_single, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -230,6 +230,9 @@ struct State {
     cudaEvent_t ev_scanned = nullptr;  // the ghost offsets scanned (the readback waits on it)
     cudaStream_t copy_stream = nullptr;  // the ghost count's readback, beside the emit kernel
     int scan_attr_device = -1;         // device whose k_scan_single shared-memory attribute is set
+    unsigned long long* lb_tiles = nullptr;  // look-back scan: one word per tile (k_neigh.cu)
+    int lb_tile_cap = 0;
+    unsigned lb_epoch = 0;             // look-back scan launches so far (tags the tile words)
     double* thermo_host = nullptr;     // pinned [kThermoSlots][4]: asynchronous thermo reads
     cudaEvent_t thermo_ev[8] = {};     // one per slot: its copy has landed
     long long thermo_slot_ticket[8] = {-1, -1, -1, -1, -1, -1, -1, -1};
