@@ -450,12 +450,14 @@ bool Comm::exchange(const std::vector<HostMsg>& sends, const std::vector<HostMsg
         size_t left;
     };
     std::vector<X> tx, rx;
+    // one message per peer and direction: two on one connection would interleave their bytes
+    std::vector<char> seen_tx(world_, 0), seen_rx(world_, 0);
     for (const HostMsg& s : sends) {
-        if (s.peer < 0 || s.peer >= world_ || s.peer == rank_) return fail("exchange: bad peer");
+        if (s.peer < 0 || s.peer >= world_ || s.peer == rank_ || seen_tx[s.peer]++) return fail("exchange: bad peer");
         if (s.bytes) tx.push_back({fd_[s.peer], static_cast<char*>(s.data), s.bytes});
     }
     for (const HostMsg& s : recvs) {
-        if (s.peer < 0 || s.peer >= world_ || s.peer == rank_) return fail("exchange: bad peer");
+        if (s.peer < 0 || s.peer >= world_ || s.peer == rank_ || seen_rx[s.peer]++) return fail("exchange: bad peer");
         if (s.bytes) rx.push_back({fd_[s.peer], static_cast<char*>(s.data), s.bytes});
     }
     const double limit = timeout_s();

@@ -291,9 +291,10 @@ class Simulation:
         return self.lib.md_get_number_of_particles(), self.lib.md_get_number_of_ghost_particles()
 
     def arrays(self):
-        """(masses, positions, velocities, forces) of the locals via md_copy_data_from_accelerator."""
+        """(masses, positions, velocities, forces) of the locals via md_copy_data_from_accelerator
+        (several ranks: this rank's current locals, whose number changes as atoms migrate)."""
         self.lib.md_copy_data_from_accelerator()
-        n = self.n
+        n = self.n = self.lib.md_get_number_of_particles()
         # every element is written by md_write_grid_data_to_arrays
         m, x, v, f = np.empty(n), np.empty((n, 3)), np.empty((n, 3)), np.empty((n, 3))
         self.lib.md_write_grid_data_to_arrays(ptr(m), ptr(x), ptr(v), ptr(f))

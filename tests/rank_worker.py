@@ -93,7 +93,6 @@ def md_mode(out, cells, steps, precision, rebuild, benchmark="default"):
     sizes = np.array([len(l) for l in tinymd.neighbor_lists(lib, sim.n)], dtype=np.int32)
     sim.step(dt, steps)
     nloc, ngh = sim.counts()
-    sim.n = nloc
     _, x1, v1, f1 = sim.arrays()
     tinymd.check(lib)
     np.savez(out, x0=x0, nb0=sizes, x=x1, v=v1, f=f1, n=nloc, g=ngh, rank=rank, box=box,
