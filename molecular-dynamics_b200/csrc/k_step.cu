@@ -329,7 +329,14 @@ __device__ __forceinline__ float mixed_del(uint32_t en, const float4& ri, const 
     dz = fmaf(a.hz, sz, ri.z - rj.z);
     return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
 }
-__device__ __forceinline__ bool mixed_fast(float rsq, const LjArgs& a) { return rsq < a.rc2_lo && rsq >= a.close2; }
+__device__ __forceinline__ bool mixed_fast(float rsq, const LjArgs& a) {
+    return fabsf(rsq - a.fast_mid) < a.fast_half;
+}
+// f/r of a pair from sr2 = 1/r^2 (five FP32 operations), and t = 1/r^6 for the energy
+__device__ __forceinline__ float mixed_force(float sr2, const LjArgs& a, float& t) {
+    t = sr2 * sr2 * sr2;
+    return (t * sr2) * fmaf(a.lj_a, t, a.lj_b);
+}
 
 // FP64 evaluation of one half-list pair of the mixed form, its reaction added to j's root
 template <bool THERMO>
@@ -393,10 +400,9 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
                 float dx, dy, dz;
                 const float rsq = mixed_del(cur[u], ri, rj[u], a, dx, dy, dz);
                 const bool fast = mixed_fast(rsq, a);
-                float sr2;
+                float sr2, t;
                 asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
-                const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
-                float f = sr6 * sr2 * fmaf(a.eps48f, sr6, a.eps24nf);
+                float f = mixed_force(sr2, a, t);
                 f = fast ? f : 0.f;
                 const float px = dx * f, py = dy * f, pz = dz * f;
                 fx += px;
@@ -404,7 +410,7 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
                 fz += pz;
                 if (fast) add_force32(frc32 + reaction_slot((int)(cur[u] >> kCodeBits), a.N, groot), -px, -py, -pz);
                 if (THERMO) {
-                    ef += fast ? a.eps4f * sr6 * (sr6 - 1.0f) : 0.f;
+                    ef += fast ? t * fmaf(a.lj_c, t, a.lj_d) : 0.f;
                     wf = fmaf(f, rsq, wf);
                     ncnt += fast ? 1 : 0;
                 }
@@ -485,16 +491,15 @@ __device__ __forceinline__ bool mixed_pair(uint32_t en, const float4& ri, const 
     float dx, dy, dz;
     const float rsq = mixed_del(en, ri, rj, a, dx, dy, dz);
     const bool fast = mixed_fast(rsq, a);
-    float sr2;
+    float sr2, t;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(sr2) : "f"(rsq));
-    const float sr6 = sr2 * sr2 * sr2 * a.sig6f;
-    float f = sr6 * sr2 * fmaf(a.eps48f, sr6, a.eps24nf);
+    float f = mixed_force(sr2, a, t);
     f = fast ? f : 0.f;
     fx = fmaf(dx, f, fx);
     fy = fmaf(dy, f, fy);
     fz = fmaf(dz, f, fz);
     if (THERMO) {
-        ef += fast ? a.eps4f * sr6 * (sr6 - 1.0f) : 0.f;
+        ef += fast ? t * fmaf(a.lj_c, t, a.lj_d) : 0.f;
         wf = fmaf(f, rsq, wf);
         ncnt += fast ? 1 : 0;
     }

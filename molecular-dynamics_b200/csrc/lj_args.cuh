@@ -12,7 +12,10 @@ struct LjArgs {
     double dt_i, h_i;          // the next step's initial integration (fused kernels only)
     double alo[3], rb_h;       // rebasing grid (mixed form's positions)
     // mixed form
-    float rc2_lo, rc2_hi, close2, sig6f, eps48f, eps4f, eps24nf;
+    float rc2_lo, rc2_hi, close2;
+    float fast_mid, fast_half;  // the FP32 window [close2, rc2_lo) as |rsq - mid| < half
+    float lj_a, lj_b;           // force: f/r = t/r^2 (lj_a t + lj_b), t = 1/r^6
+    float lj_c, lj_d;           // energy: t (lj_c t + lj_d)
     float hx, hy, hz;  // shift decode scales (see the kernels)
     // a launch on lists whose build status is still in flight: the kernel returns without
     // writing when that build overflowed the capacity or left locals outside the grid
@@ -59,10 +62,16 @@ inline LjArgs lj_args(const State& s, const PendingForce& p, double dt) {
     // 1.02 sigma, 4.5e-6 / 4.7e-6 after 220 / 1000 steps with 1.04 sigma (~1.0 FP64 pair per
     // atom) and 5.7e-6 / 3.9e-6 / 3.8e-6 with 1.05 sigma (~1.2-1.4 FP64 pairs per atom)
     a.close2 = (float)((1.04 * p.sigma) * (1.04 * p.sigma));
-    a.sig6f = (float)a.sigma6;
-    a.eps48f = (float)(48.0 * p.eps);
-    a.eps24nf = (float)(-24.0 * p.eps);
-    a.eps4f = (float)(4.0 * p.eps);
+    // one comparison of |rsq - mid| instead of two: its edges move by an ulp at most, and a pair
+    // on either side of an edge is exact enough in both forms (both edges are margins)
+    a.fast_mid = (float)(0.5 * ((double)a.rc2_lo + (double)a.close2));
+    a.fast_half = (float)(0.5 * ((double)a.rc2_lo - (double)a.close2));
+    // with t = 1/r^6: sr6 = sigma^6 t, f/r = 48 eps sr6 (sr6 - 1/2) / r^2 = t/r^2 (A t + B) and
+    // 4 eps sr6 (sr6 - 1) = t (C t + D)
+    a.lj_a = (float)(48.0 * p.eps * a.sigma6 * a.sigma6);
+    a.lj_b = (float)(-24.0 * p.eps * a.sigma6);
+    a.lj_c = (float)(4.0 * p.eps * a.sigma6 * a.sigma6);
+    a.lj_d = (float)(-4.0 * p.eps * a.sigma6);
     a.hx = a.hy = a.hz = 0.0f;
     return a;
 }
