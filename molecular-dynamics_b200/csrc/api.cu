@@ -319,11 +319,14 @@ bool grow_atoms(State& s, int need) {
 
 // list capacity in entries per atom, a multiple of four (the list is stored in quads)
 int list_rows(int rows) { return (std::max(rows, 4) + 3) & ~3; }
+// entries allocated for the lists: one quad row more than the capacity, which the mixed force
+// kernels read ahead into after an atom's last quad (the row is never used)
+size_t list_entries(const State& s) { return (size_t)(s.nb_cap + 4) * s.nb_stride; }
 
 void grow_lists(State& s, int rows) {
     dfree(&s.nbl);
     s.nb_cap = list_rows(rows);
-    dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+    dalloc(&s.nbl, list_entries(s));
     s.lists_valid = 0;
 }
 
@@ -335,7 +338,7 @@ bool ensure_locals(State& s, int n) {
     if (n > s.nb_stride) {
         s.nb_stride = ((n + n / 8 + 31) / 32) * 32;
         dfree(&s.nbl);
-        dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+        dalloc(&s.nbl, list_entries(s));
         dfree(&s.bmask);
         dalloc(&s.bmask, (size_t)s.nb_stride);
         dfree(&s.bcount);
@@ -361,7 +364,7 @@ bool allocate_state(State& s, int N, int nb_cap) {
     const int nblk = border_blocks(s.nb_stride);
     dalloc(&s.bcount, (size_t)2 * 27 * nblk + 1);  // border types (26) or migration classes (27), scanned
     s.nb_cap = list_rows(nb_cap > 0 ? nb_cap : 100);
-    dalloc(&s.nbl, (size_t)s.nb_cap * s.nb_stride);
+    dalloc(&s.nbl, list_entries(s));
     if (!s.ev_counted) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_counted, cudaEventDisableTiming));
     if (!s.ev_scanned) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_scanned, cudaEventDisableTiming));
     if (!s.ev_status) TMD_CUDA(cudaEventCreateWithFlags(&s.ev_status, cudaEventDisableTiming));

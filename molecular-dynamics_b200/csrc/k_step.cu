@@ -393,7 +393,7 @@ k_lj_mixed_half(const float4* __restrict__ pos32, const double4* __restrict__ po
             float4 rj[kB32];
 #pragma unroll
             for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (cur[u] >> kCodeBits));
-            eq = list_quad(nbl, min(b + 1, nquad - 1), i, a.stride);
+            eq = list_quad(nbl, b + 1, i, a.stride);  // the last read lands in the spare row
             unsigned slow = 0;
 #pragma unroll
             for (int u = 0; u < kB32; ++u) {
@@ -543,7 +543,7 @@ k_lj_mixed_bf(const float4* __restrict__ pos32, const double4* __restrict__ pos,
 #pragma unroll
             for (int u = 0; u < kB32; ++u) rj[u] = __ldg(pos32 + (cur[u] >> kCodeBits));
             // the next quad loads while this one's gathers are in flight
-            eq = list_quad(nbl, min(b + 1, nquad - 1), i, a.stride);
+            eq = list_quad(nbl, b + 1, i, a.stride);  // the last read lands in the spare row
             unsigned slow = 0;
 #pragma unroll
             for (int u = 0; u < kB32; ++u)
