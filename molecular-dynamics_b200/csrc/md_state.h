@@ -111,9 +111,14 @@ constexpr int kImgW = kImg1 + kImg2;
 
 constexpr int kThermoSlots = 8;  // asynchronous thermo reads in flight at most
 
-// threads per block of the ghost count and emit kernels: the ghost offsets are scanned over
-// 26 types x blocks, so larger blocks make that scan shorter
-constexpr int kBorderThreads = 1024;
+// threads per block of the ghost count and emit kernels (and the migration's): the ghost offsets
+// are scanned over 26 types x blocks, 13k values at 131k atoms, one look-back scan; 1,024-thread
+// blocks kept that scan to 3.3k values for the one-block scan, but the emit runs a single
+// half-occupied wave then (rebuild step 195 -> 192-193.5 us with 256)
+#ifndef TMD_BORDER_THREADS
+#define TMD_BORDER_THREADS 256
+#endif
+constexpr int kBorderThreads = TMD_BORDER_THREADS;
 inline int border_blocks(int N) { return (N + kBorderThreads - 1) / kBorderThreads; }
 
 // Multi-rank runs (comm.h): the images this rank sends into its neighbours' regions and the
