@@ -683,7 +683,7 @@ int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D
     if (cm.active()) {
         // several ranks: the layout of md_get_node_bounding_box (made here from the world box
         // when the caller skipped it); every divided axis must hold a full halo per rank
-        if (!cm.topo_set) {
+        if (!cm.topo_set || cm.topo.world != cm.world() || cm.topo.rank != cm.rank()) {
             double len[3];
             int dims[3];
             for (int d = 0; d < 3; ++d) len[d] = aabb[2 * d + 1] - aabb[2 * d];

@@ -415,6 +415,7 @@ bool Comm::init() {
     }
     world_ = w;
     rank_ = r;
+    topo_set = false;  // a layout made before the ranks connected was a one-rank layout
     if (use_nccl == 1) {
         ncclComm_t c = nullptr;
         const ncclResult_t e = g_nccl.init_rank(&c, w, uid, r);
