@@ -9,6 +9,10 @@
         configuration): setup inside the rank box, velocities, borders, lists, forces, STEPS
         timesteps with reneighbouring every REBUILD steps; saves the locals and the neighbour
         counts of the first lists.
+    python tests/rank_worker.py leave OUT.json CELLS
+        the last rank leaves after 5 steps; the others record the error of their next steps.
+    python tests/rank_worker.py half OUT.json CELLS
+        half lists on several ranks: the error md_assemble_neighborlists latches.
     python tests/rank_worker.py nccl BYTES
         the NCCL binding on this process's GPU alone (tmd_comm_nccl_selftest).
     python tests/rank_worker.py perf OUT.json CELLS STEPS REBUILD PRECISION
@@ -101,6 +105,70 @@ def md_mode(out, cells, steps, precision, rebuild, benchmark="default"):
     lib.md_mpi_finalize()
 
 
+def leave_mode(out, cells):
+    """Failure detection without a GPU fault: every rank runs 5 steps of the 8^3-style lattice;
+    then the last rank waits for its device work and leaves (the process ends, its connections
+    close) while the others try 20 more steps.  Their next halo exchange fails on the host and
+    latches MD_ERR_COMM; they return instead of waiting for the missing rank."""
+    import time
+    lib = tinymd.load(build_if_missing=False)
+    lib.md_mpi_initialize()
+    tinymd.check(lib)
+    rank, world_size = lib.md_get_world_rank(), lib.md_get_world_size()
+    grid = np.array([cells] * 3, dtype=np.int32)
+    world, a1, a2 = np.zeros(6), np.zeros(6), np.zeros(6)
+    assert lib.tmd_setup_world(0, ptr(grid), 1.6796, ptr(world), ptr(a1), ptr(a2)) == 0
+    box = np.zeros(6)
+    lib.md_get_node_bounding_box(ptr(world), ptr(box))
+    n = lib.tmd_setup_generate(0, ptr(world), ptr(box), ptr(a1), ptr(a2), 1.6796)
+    m, x, v = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3))
+    lib.tmd_setup_fetch(ptr(m), ptr(x), ptr(v))
+    sim = tinymd.Simulation(lib, m, x, v, world, box, temp=1.44, reneigh=10)
+    sim.step(0.005, 5)
+    lib.md_synchronize()  # nothing of this rank in flight on the GPU
+    if rank == world_size - 1:
+        os._exit(0)  # leaves between steps, without finalising
+    t0 = time.perf_counter()
+    for _ in range(20):
+        lib.md_initial_integration(0.005)
+        lib.md_synchronize_ghost_layer()
+        lib.md_compute_lennard_jones(False, 2.5, 1.0, 1.0)
+        lib.md_final_integration(0.005)
+    lib.md_synchronize()
+    res = {"rank": rank, "err": lib.md_last_error(), "msg": lib.md_last_error_string().decode(),
+           "seconds": time.perf_counter() - t0}
+    with open(out, "w") as f:
+        json.dump(res, f)
+    lib.md_deallocate_grid()
+
+
+def half_mode(out, cells):
+    """Half lists on several ranks: md_assemble_neighborlists(half) latches MD_ERR_UNSUPPORTED."""
+    lib = tinymd.load(build_if_missing=False)
+    lib.md_mpi_initialize()
+    tinymd.check(lib)
+    grid = np.array([cells] * 3, dtype=np.int32)
+    world, a1, a2 = np.zeros(6), np.zeros(6), np.zeros(6)
+    assert lib.tmd_setup_world(0, ptr(grid), 1.6796, ptr(world), ptr(a1), ptr(a2)) == 0
+    box = np.zeros(6)
+    lib.md_get_node_bounding_box(ptr(world), ptr(box))
+    n = lib.tmd_setup_generate(0, ptr(world), ptr(box), ptr(a1), ptr(a2), 1.6796)
+    m, x, v = np.zeros(n), np.zeros((n, 3)), np.zeros((n, 3))
+    lib.tmd_setup_fetch(ptr(m), ptr(x), ptr(v))
+    keep = [np.ascontiguousarray(a) for a in (m, x, v)]
+    lib.md_initialize_grid(ptr(keep[0]), ptr(keep[1]), ptr(keep[2]), n, ptr(world), ptr(box), 2.8, 60, 100)
+    lib.md_copy_data_to_accelerator()
+    lib.md_exchange_particles()
+    lib.md_borders()
+    lib.md_distribute_particles()
+    lib.md_assemble_neighborlists(True, 2.8)
+    res = {"err": lib.md_last_error(), "msg": lib.md_last_error_string().decode()}
+    with open(out, "w") as f:
+        json.dump(res, f)
+    lib.md_deallocate_grid()
+    lib.md_mpi_finalize()
+
+
 def perf_mode(out, cells, steps, rebuild, precision):
     """The LJ lattice split over the ranks, timed through md_run_timesteps (host clock, after
     warm-up), with the device phase split and this rank's halo size."""
@@ -149,6 +217,10 @@ if __name__ == "__main__":
         rc = tinymd.load(build_if_missing=False).tmd_comm_nccl_selftest(int(sys.argv[2]))
         print("nccl selftest", rc)
         sys.exit(0 if rc == 0 else 1)
+    elif sys.argv[1] == "leave":
+        leave_mode(sys.argv[2], int(sys.argv[3]))
+    elif sys.argv[1] == "half":
+        half_mode(sys.argv[2], int(sys.argv[3]))
     elif sys.argv[1] == "perf":
         perf_mode(sys.argv[2], int(sys.argv[3]), int(sys.argv[4]), int(sys.argv[5]), int(sys.argv[6]))
     else:

@@ -13,6 +13,8 @@ of one waits for another's).  The oracle runs the same setup as one box with exa
 * The contact-fixed DEM model on two ranks (the halo carries velocities) matches likewise.
 * The mixed form on four ranks stays close to the same run (a sanity bound over 100 steps).
 * The reference's own driver (main.cpp, unmodified, linked to the product) runs on two ranks.
+* A rank that leaves between steps is detected by the others (MD_ERR_COMM, no hang); half
+  lists on several ranks are refused.
 """
 import os
 import subprocess
@@ -176,6 +178,33 @@ def test_mixed_form_on_four_ranks(one_box, tmp_path):
     assert d.max() < 1e-3
     rms = np.sqrt(np.mean(one_box["f"] ** 2))
     assert np.max(np.abs(f - one_box["f"][i])) / rms < 1e-2
+
+
+def test_a_rank_that_leaves_is_detected(tmp_path):
+    """Failure detection without a GPU fault: after 5 steps the last of three ranks waits for
+    its device work and exits between steps.  The other two find the closed connections at
+    their next halo exchange: MD_ERR_COMM is latched, and they finish their remaining steps
+    in far less than the exchange timeout instead of waiting for the missing rank."""
+    import json
+    outs = run_ranks(3, [sys.executable, WORKER, "leave", str(tmp_path / "r{rank}.json"), "8"],
+                     {"TINYMD_COMM": "socket", "TINYMD_DEVICE": "0", "TINYMD_COMM_TIMEOUT": "30"}, timeout=300)
+    for rc, out in outs:
+        assert rc == 0, out
+    for r in range(2):
+        x = json.load(open(tmp_path / f"r{r}.json"))
+        assert x["err"] == 7, x
+        assert x["seconds"] < 25.0
+
+
+def test_half_lists_on_several_ranks_are_refused(tmp_path):
+    import json
+    outs = run_ranks(2, [sys.executable, WORKER, "half", str(tmp_path / "r{rank}.json"), "8"],
+                     {"TINYMD_COMM": "socket", "TINYMD_DEVICE": "0"}, timeout=300)
+    for rc, out in outs:
+        assert rc == 0, out
+    for r in range(2):
+        x = json.load(open(tmp_path / f"r{r}.json"))
+        assert x["err"] == 4 and "half lists" in x["msg"]
 
 
 def test_nccl_binding_on_one_gpu():
