@@ -15,6 +15,8 @@
 #include <deque>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "comm.h"
 #include "md_common.cuh"
 #include "md_state.h"
@@ -23,6 +25,14 @@
 namespace tmd {
 
 State g_state;
+
+// An NVTX range over an entry point that enqueues work, so a profiler's timeline (nsys, or
+// `ncu --nvtx`) groups the kernels by the md_* call that issued them.  NVTX is header-only here:
+// without an attached tool a range costs a pointer test.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 
 // ---------------------------------------------------------------------------
 // errors, launches, memory
@@ -666,6 +676,7 @@ void md_set_stream(void* stream) {
 int md_initialize_grid(double const* masses, Vector3D const* positions, Vector3D const* velocities, int n,
                        double const* aabb, double const* rank_aabb, double cell_spacing, int cell_capacity,
                        int neighborlist_capacity) {
+    Range range("md_initialize_grid");
     (void)cell_capacity;  // cells are a counting sort here: no per-cell capacity
     State& s = g_state;
     int ndev = 0;
@@ -794,6 +805,7 @@ void md_create_velocity(double t_request) {
 
 // core/grid.impala:360-367
 void md_copy_data_to_accelerator(void) {
+    Range range("md_copy_data_to_accelerator");
     State& s = g_state;
     if (!require_alive("md_copy_data_to_accelerator")) return;
     flush_all(s);
@@ -822,6 +834,7 @@ void md_copy_data_to_accelerator(void) {
 // when a reader needs it, and then only the part it needs: md_write_grid_data_to_arrays takes
 // the locals straight into the caller's arrays.
 void md_copy_data_from_accelerator(void) {
+    Range range("md_copy_data_from_accelerator");
     State& s = g_state;
     if (!require_alive("md_copy_data_from_accelerator")) return;
     flush_all(s);
@@ -845,6 +858,7 @@ void md_copy_data_from_accelerator(void) {
 // comm/comm.impala:392-525: with one rank nothing leaves (the periodic wrap is md_enforce_pbc's);
 // with several, locals beyond the rank box move to their new owner (k_halo.cu)
 void md_exchange_particles(void) {
+    Range range("md_exchange_particles");
     State& s = g_state;
     if (!require_alive("md_exchange_particles")) return;
     flush_locals(s);
@@ -856,6 +870,7 @@ void md_exchange_particles(void) {
 }
 
 void md_enforce_pbc(void) {  // wraps locals only: a pending ghost carry stays pending
+    Range range("md_enforce_pbc");
     State& s = g_state;
     if (!require_alive("md_enforce_pbc")) return;
     flush_locals(s);
@@ -863,6 +878,7 @@ void md_enforce_pbc(void) {  // wraps locals only: a pending ghost carry stays p
 }
 
 void md_borders(void) {
+    Range range("md_borders");
     State& s = g_state;
     if (!require_alive("md_borders")) return;
     s.pend_ghost = false;  // every ghost is written anew below: the carry would be overwritten
@@ -874,6 +890,7 @@ void md_borders(void) {
 }
 
 void md_distribute_particles(void) {
+    Range range("md_distribute_particles");
     State& s = g_state;
     if (!require_alive("md_distribute_particles")) return;
     flush_all(s);
@@ -882,6 +899,7 @@ void md_distribute_particles(void) {
 }
 
 void md_assemble_neighborlists(bool half, double cutoff) {
+    Range range("md_assemble_neighborlists");
     State& s = g_state;
     if (!require_alive("md_assemble_neighborlists")) return;
     if (half && s.halo.on) {
@@ -902,6 +920,7 @@ void md_assemble_neighborlists(bool half, double cutoff) {
 }
 
 void md_initial_integration(double dt) {
+    Range range("md_initial_integration");
     State& s = g_state;
     if (!require_alive("md_initial_integration")) return;
     if (s.pend_final && !s.pend_ghost && !s.pend_init && !s.pend_force.valid) {
@@ -923,6 +942,7 @@ void md_initial_integration(double dt) {
 }
 
 void md_synchronize_ghost_layer(void) {
+    Range range("md_synchronize_ghost_layer");
     State& s = g_state;
     if (!require_alive("md_synchronize_ghost_layer")) return;
     resolve_lists(s);
@@ -955,6 +975,7 @@ void md_synchronize_ghost_layer(void) {
 }
 
 void md_compute_lennard_jones(bool half, double rc, double eps, double sigma) {
+    Range range("md_compute_lennard_jones");
     State& s = g_state;
     if (!require_alive("md_compute_lennard_jones")) return;
     flush_all(s, false);
@@ -973,6 +994,7 @@ void md_compute_lennard_jones(bool half, double rc, double eps, double sigma) {
 }
 
 void md_compute_dem(bool half, double rc, double damping_n, double damping_t, double stiffness, double friction) {
+    Range range("md_compute_dem");
     State& s = g_state;
     if (!require_alive("md_compute_dem")) return;
     flush_all(s, false);
@@ -990,6 +1012,7 @@ void md_compute_dem(bool half, double rc, double damping_n, double damping_t, do
 }
 
 void md_final_integration(double dt) {
+    Range range("md_final_integration");
     State& s = g_state;
     if (!require_alive("md_final_integration")) return;
     flush_links(s);
@@ -1546,6 +1569,7 @@ __global__ void k_l2_read(const uint4* __restrict__ b, size_t n, unsigned* __res
 // The md driver's timestep loop (main.cpp:715-776) issued natively.
 int md_run_timesteps(int steps, double dt, int reneigh_every, int step0, double list_cutoff, float* step_ms,
                      void* flush_buf, long long flush_bytes) {
+    Range range("md_run_timesteps");
     State& s = g_state;
     if (!require_alive("md_run_timesteps")) return -1;
     if (!s.force_cfg.valid || reneigh_every <= 0 || steps < 0) {
